@@ -1,0 +1,313 @@
+#!/usr/bin/env python3
+"""Benchmark: Msamples/s of the B200 path tracer on the material-divergent scene.
+
+Workload (one step = one full render): "icospheres" -- ground quad + 512 level-2 icospheres
+(163,844 triangles, Lambertian / mirror / dielectric materials) under an emissive quad -- at
+1280x720, 64 spp, max depth 8, seed 1234 (58,982,400 path samples per step). Synthetic scene
+built by the engine's generator; no external data.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--arm megakernel|wavefront]
+  python bench.py --impl reference ...   # the reference's own CPU arm on the host cores
+
+N > 1 runs N independent replicas (one process per GPU under torchrun): the path has no
+cross-GPU exchange, value = all samples rendered / max-over-ranks device time.
+Rank 0 prints one JSON line.
+"""
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "graphics-book-tutorials_b200")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+PROFILE_DIR = os.path.join(ROOT, "profiles")
+
+SCENE, WIDTH, HEIGHT, SPP, DEPTH, SEED = "icospheres", 1280, 720, 64, 8, 1234
+WORKLOAD = f"{SCENE}-512 {WIDTH}x{HEIGHT} {SPP}spp depth{DEPTH} seed{SEED}"
+METRIC = "Msamples/s per scene vs plain megakernel (bit-equal image); served p50/p99 latency"
+
+
+def load_engine():
+    spec = importlib.util.spec_from_file_location("wfb200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["wfb200"] = mod
+    spec.loader.exec_module(mod)
+    mod.load_library()
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, ORACLE_DIR)
+    import oracle  # noqa: E402
+    return oracle
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples taken during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def read_profile_traffic():
+    """DRAM bytes per path sample of the megakernel from the committed ncu summary, if present."""
+    path = os.path.join(PROFILE_DIR, "megakernel_icospheres.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_sample:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def dist_setup(n_gpus):
+    if n_gpus <= 1 and "WORLD_SIZE" not in os.environ:
+        return None, 0, 1, 0
+    import torch.distributed as dist
+    import datetime
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist, rank, world, local
+
+
+def run_reference(args):
+    """Reference CPU arm (render_cpu compiled from the reference sources) on this host's cores."""
+    dist, rank, world, _ = dist_setup(args.gpus)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    orc = load_oracle()
+    wfb = load_engine()
+    arrays = wfb.Scene.generate(SCENE, WIDTH, HEIGHT, SEED, 16).export()
+    threads = os.cpu_count() or 1
+    sample_spp = args.ref_spp
+    kind = "reference" if orc.reference_available() else "port"
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        if kind == "reference":
+            orc.ref_render_cpu(arrays, sample_spp, SEED, DEPTH, threads)
+        else:
+            orc.render_sums(arrays, sample_spp, SEED, DEPTH, threads=threads)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    samples = WIDTH * HEIGHT * sample_spp
+    value = samples * len(times) / sum(times) / 1e6
+    sample_desc = f"{WIDTH}x{HEIGHT} at {sample_spp} spp of the {SPP}-spp workload per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Msamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "arm": "reference render_cpu (WVM/src/cpu_renderer.cpp:13)",
+                   "sample": sample_desc, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Msamples/s", "cores": threads, "kind": kind,
+                         "sample": sample_desc},
+        "e2e": {"value": round(value, 4), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(wfb, seconds_target=12.0):
+    """Reference CPU arm (or the oracle port) on a bounded sample of the workload, all host threads."""
+    orc = load_oracle()
+    arrays = wfb.Scene.generate(SCENE, WIDTH, HEIGHT, SEED, 16).export()
+    threads = os.cpu_count() or 1
+    kind = "reference" if orc.reference_available() else "port"
+    spp = 1
+    t0 = time.perf_counter()
+    if kind == "reference":
+        orc.ref_render_cpu(arrays, spp, SEED, DEPTH, threads)
+    else:
+        orc.render_sums(arrays, spp, SEED, DEPTH, threads=threads)
+    dt = time.perf_counter() - t0
+    spp2 = max(1, min(SPP, int(seconds_target / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    if kind == "reference":
+        orc.ref_render_cpu(arrays, spp2, SEED, DEPTH, threads)
+    else:
+        orc.render_sums(arrays, spp2, SEED, DEPTH, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": round(WIDTH * HEIGHT * spp2 / dt / 1e6, 4), "unit": "Msamples/s", "cores": threads,
+            "kind": kind, "sample": f"{WIDTH}x{HEIGHT} at {spp2} spp (of {SPP}), seed {SEED}, depth {DEPTH}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--arm", default="megakernel", choices=["megakernel", "wavefront"])
+    ap.add_argument("--ref-spp", type=int, default=2, help="samples per pixel of one reference-arm step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    dist, rank, world, local = dist_setup(args.gpus)
+    import torch
+    torch.cuda.set_device(local)
+    wfb = load_engine()
+    mode = wfb.MEGAKERNEL if args.arm == "megakernel" else wfb.WAVEFRONT
+    scene = wfb.Scene.generate(SCENE, WIDTH, HEIGHT, SEED, 16)
+    host_arrays = scene.export()
+    renderer = wfb.GpuRenderer(scene, mode)
+    params = wfb.RenderParams(spp=SPP, seed=SEED, max_depth=DEPTH)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    # untimed counting run: rays per sample for the roofline bytes model
+    cst = wfb.RenderStats()
+    ref_img = renderer.render(wfb.RenderParams(spp=SPP, seed=SEED, max_depth=DEPTH, count_rays=True), cst)
+    samples = WIDTH * HEIGHT * SPP
+    ext_ps, sh_ps = cst.extension_rays / samples, cst.shadow_rays / samples
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        renderer.render(params)
+    clocks = ClockSampler(torch.cuda.current_device())
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    dev_ms = []
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush outside the event-timed region
+        torch.cuda.synchronize()
+        st = wfb.RenderStats()
+        img = renderer.render(params, st)  # render_ms: CUDA events on the launching stream
+        dev_ms.append(st.render_ms)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = float(sum(dev_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    assert np.array_equal(img.rgb.view(np.uint32), ref_img.rgb.view(np.uint32)), "render is not deterministic"
+    value = samples * args.steps * world / (total_ms / 1e3) / 1e6
+    ms_per_step = total_ms / args.steps
+
+    # e2e through the public API: host arrays -> scene upload -> render -> film back in host memory
+    e2e_times = []
+    h2d = d2h = 0
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = wfb.Scene.from_arrays(host_arrays)
+        r2 = wfb.GpuRenderer(s2, mode)
+        out = r2.render(params)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_times.append(dt)
+        h2d = s2.device_bytes()
+        d2h = 5 * WIDTH * HEIGHT * 4  # film sums rgb + lum + lum2
+        r2.close()
+        s2.close()
+    e2e_s = sum(e2e_times) / len(e2e_times)
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = samples * world / e2e_s / 1e6
+
+    peaks, peak_kind = measured_peaks()
+    bytes_per_sample = 224.0 * ext_ps + 96.0 * sh_ps + 40.0
+    achieved = samples * bytes_per_sample / (ms_per_step / 1e3) / 1e9
+    traffic_ps = read_profile_traffic()
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "arm": args.arm, "parallelism": f"replicas{world}" if world > 1 else "1gpu",
+                   "l2": "flushed (256 MB write) before every timed step", "scene_hash": "%016x" % scene.hash()},
+        "roofline": {
+            "bound": "hbm", "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": round(achieved / peaks["hbm_gbs"], 4),
+            "traffic": round(traffic_ps * samples) if traffic_ps else None,
+            "peak_source": peak_kind,
+            "bytes_model": "224*ext + 96*shadow + 40 B per sample (path-state bytes a wavefront moves)",
+            "ext_rays_per_sample": round(ext_ps, 4), "shadow_rays_per_sample": round(sh_ps, 4),
+            "kernel": "megakernel_persistent" if args.arm == "megakernel" else "wavefront_persistent",
+        },
+        "e2e": {"value": round(e2e_value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": args.steps,
+        "mrays_per_s": round((ext_ps + sh_ps) * value, 2),
+        "clocks": clk,
+        "device": wfb.device_name(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wfb)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del flush
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

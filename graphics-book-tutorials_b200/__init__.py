@@ -1,0 +1,399 @@
+"""Python host side of the B200 path-tracing engine (ctypes over the C ABI in include/wfb200.h).
+
+Mirrors the reference's C++ renderer interface (WVM/include/wf/renderer.hpp:11-74 in
+us-llm-engineer/graphics-book-tutorials): ``GpuRenderer(scene, mode)`` with ``render``,
+``reset``, ``run_passes``, ``download``, ``download_mean``, ``device_bytes``; ``RenderParams`` and
+``RenderStats`` with the reference's field names; errors are raised as ``WfbError`` carrying the
+C status code (the reference raises ``std::runtime_error``).
+
+There is no CPU fallback: importing this module requires the built ``libwfb200.so`` next to it
+(``make -C graphics-book-tutorials_b200``) and every render runs the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwfb200.so")
+
+# ---- status codes (include/wfb200.h) ----
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_CUDA = 2
+ERR_OUT_OF_MEMORY = 3
+ERR_NOT_FINALIZED = 4
+ERR_UNSUPPORTED = 5
+ERR_TIMEOUT = 6
+ERR_DEVICE_WAIT = 7
+ERR_INTERNAL = 8
+
+MEGAKERNEL = 0
+WAVEFRONT = 1
+
+# ---- reference struct layouts as numpy dtypes (WVM/include/wf/scene.hpp:12-100) ----
+VEC3 = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4")])
+SPHERE = np.dtype([("center", "<f4", 3), ("radius", "<f4"), ("material", "<i4"), ("pad", "<i4", 3)])
+TRIANGLE = np.dtype([("i0", "<i4"), ("i1", "<i4"), ("i2", "<i4"), ("material", "<i4")])
+MATERIAL = np.dtype([("type", "<i4"), ("ior", "<f4"), ("pad0", "<f4"), ("pad1", "<f4"),
+                     ("albedo", "<f4", 3), ("pad2", "<f4"), ("emission", "<f4", 3), ("pad3", "<f4")])
+BVH_NODE = np.dtype([("lo", "<f4", 3), ("skip", "<i4"), ("hi", "<f4", 3), ("prim_start", "<i4"),
+                     ("prim_count", "<i4"), ("pad", "<i4", 3)])
+LIGHT = np.dtype([("prim", "<i4"), ("area", "<f4"), ("pad", "<f4", 2)])
+RAY = np.dtype([("o", "<f4", 3), ("tmin", "<f4"), ("d", "<f4", 3), ("tmax", "<f4")])
+HIT = np.dtype([("t", "<f4"), ("prim", "<i4"), ("u", "<f4"), ("v", "<f4")])
+assert SPHERE.itemsize == 32 and MATERIAL.itemsize == 48 and BVH_NODE.itemsize == 48
+
+
+class WfbError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[wfb status {status}] {message}")
+        self.status = status
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("spheres", ctypes.c_void_p), ("n_spheres", ctypes.c_int),
+        ("vertices", ctypes.c_void_p), ("n_vertices", ctypes.c_int),
+        ("triangles", ctypes.c_void_p), ("n_triangles", ctypes.c_int),
+        ("materials", ctypes.c_void_p), ("n_materials", ctypes.c_int),
+        ("nodes", ctypes.c_void_p), ("n_nodes", ctypes.c_int),
+        ("prim_order", ctypes.c_void_p), ("n_prim_order", ctypes.c_int),
+        ("lights", ctypes.c_void_p), ("n_lights", ctypes.c_int),
+        ("env", ctypes.c_float * 3),
+        ("cam_position", ctypes.c_float * 3), ("cam_look_at", ctypes.c_float * 3),
+        ("cam_up", ctypes.c_float * 3), ("cam_vfov_deg", ctypes.c_float),
+        ("width", ctypes.c_int), ("height", ctypes.c_int),
+    ]
+
+
+class SceneInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_spheres", ctypes.c_int), ("n_vertices", ctypes.c_int), ("n_triangles", ctypes.c_int),
+        ("n_materials", ctypes.c_int), ("n_nodes", ctypes.c_int), ("n_prim_order", ctypes.c_int),
+        ("n_lights", ctypes.c_int), ("width", ctypes.c_int), ("height", ctypes.c_int),
+        ("env", ctypes.c_float * 3), ("cam_position", ctypes.c_float * 3),
+        ("cam_look_at", ctypes.c_float * 3), ("cam_up", ctypes.c_float * 3),
+        ("cam_vfov_deg", ctypes.c_float),
+    ]
+
+
+class _CRenderParams(ctypes.Structure):
+    _fields_ = [("spp", ctypes.c_int), ("seed", ctypes.c_uint32), ("max_depth", ctypes.c_int),
+                ("count_rays", ctypes.c_int), ("stage_timing", ctypes.c_int),
+                ("queue_capacity", ctypes.c_int)]
+
+
+class _CRenderStats(ctypes.Structure):
+    _fields_ = [("render_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+                ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("queue_high_water", ctypes.c_int64 * 5), ("queue_overflows", ctypes.c_int64),
+                ("invalid_hits", ctypes.c_int64), ("peak_vram_bytes", ctypes.c_uint64),
+                ("stage_ms", ctypes.c_double * 8)]
+
+
+STAGE_NAMES = ("extend", "classify", "shade_lambert", "shade_metal", "shade_dielectric", "shadow",
+               "compact", "other")
+
+
+@dataclass
+class RenderParams:
+    """wf::RenderParams (WVM/include/wf/renderer.hpp:11-21)."""
+    spp: int = 64
+    seed: int = 1234
+    max_depth: int = 8
+    threads: int = 0
+    count_rays: bool = False
+    stage_timing: bool = False
+    queue_capacity: int = 0
+
+    def _c(self) -> _CRenderParams:
+        return _CRenderParams(int(self.spp), int(self.seed) & 0xFFFFFFFF, int(self.max_depth),
+                              int(bool(self.count_rays)), int(bool(self.stage_timing)),
+                              int(self.queue_capacity))
+
+
+@dataclass
+class RenderStats:
+    """wf::RenderStats (WVM/include/wf/renderer.hpp:23-37)."""
+    render_ms: float = 0.0
+    total_ms: float = 0.0
+    extension_rays: int = 0
+    shadow_rays: int = 0
+    queue_high_water: list = field(default_factory=lambda: [0] * 5)
+    queue_overflows: int = 0
+    invalid_hits: int = 0
+    peak_vram_bytes: int = 0
+    stages: dict = field(default_factory=dict)
+
+    @classmethod
+    def _from_c(cls, c: _CRenderStats) -> "RenderStats":
+        return cls(c.render_ms, c.total_ms, int(c.extension_rays), int(c.shadow_rays),
+                   [int(v) for v in c.queue_high_water], int(c.queue_overflows), int(c.invalid_hits),
+                   int(c.peak_vram_bytes), {n: float(c.stage_ms[i]) for i, n in enumerate(STAGE_NAMES)})
+
+
+@dataclass
+class RenderResult:
+    """wf::RenderResult (WVM/include/wf/film.hpp:11-15): rgb (h, w, 3) and lum_var (h, w)."""
+    width: int
+    height: int
+    spp: int
+    rgb: np.ndarray
+    lum_var: np.ndarray
+
+
+_lib = None
+
+
+def _ptr(a) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libwfb200.so once; raises if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C {_HERE}`")
+    lib = ctypes.CDLL(path)
+    vp, ip, i32, u32, u64 = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64
+    sig = {
+        "wfb_abi_version": (i32, []),
+        "wfb_last_error": (ctypes.c_char_p, []),
+        "wfb_device_name": (i32, [ctypes.c_char_p, i32]),
+        "wfb_scene_create": (i32, [ctypes.POINTER(SceneDesc), i32, ctypes.POINTER(vp)]),
+        "wfb_scene_generate": (i32, [ctypes.c_char_p, i32, i32, u32, i32, ctypes.POINTER(vp)]),
+        "wfb_scene_info_get": (i32, [vp, ctypes.POINTER(SceneInfo)]),
+        "wfb_scene_export": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
+        "wfb_scene_hash": (u64, [vp]),
+        "wfb_scene_validate_bvh": (i32, [vp, ctypes.c_char_p, i32]),
+        "wfb_scene_destroy": (i32, [vp]),
+        "wfb_scene_device_bytes": (u64, [vp]),
+        "wfb_renderer_create": (i32, [vp, i32, ctypes.POINTER(vp)]),
+        "wfb_renderer_set_camera": (i32, [vp, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                          ctypes.POINTER(ctypes.c_float), ctypes.c_float, i32, i32]),
+        "wfb_renderer_reset": (i32, [vp]),
+        "wfb_renderer_run_passes": (i32, [vp, i32, i32, ctypes.POINTER(_CRenderParams), ctypes.POINTER(_CRenderStats)]),
+        "wfb_renderer_download": (i32, [vp, i32, vp, vp]),
+        "wfb_renderer_download_mean": (i32, [vp, i32, vp]),
+        "wfb_renderer_download_sums": (i32, [vp, vp, vp, vp]),
+        "wfb_renderer_render": (i32, [vp, ctypes.POINTER(_CRenderParams), ctypes.POINTER(_CRenderStats), vp, vp]),
+        "wfb_renderer_device_bytes": (u64, [vp]),
+        "wfb_renderer_width": (i32, [vp]),
+        "wfb_renderer_height": (i32, [vp]),
+        "wfb_renderer_destroy": (i32, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != OK:
+        raise WfbError(status, (load_library().wfb_last_error() or b"").decode())
+
+
+def device_name() -> str:
+    buf = ctypes.create_string_buffer(256)
+    _check(load_library().wfb_device_name(buf, 256))
+    return buf.value.decode()
+
+
+class Scene:
+    """A finalized scene (wf::Scene, WVM/include/wf/scene.hpp:85-100) owned by the engine."""
+
+    def __init__(self, handle: int):
+        self._h = ctypes.c_void_p(handle)
+
+    @classmethod
+    def generate(cls, name: str, width: int, height: int, seed: int = 1234, sah_bins: int = 16) -> "Scene":
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.wfb_scene_generate(name.encode(), width, height, seed & 0xFFFFFFFF, sah_bins, ctypes.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_arrays(cls, arrays: dict, finalize_bins: int = 0) -> "Scene":
+        """arrays: dict from ``export()`` (reference dtypes) plus env/camera/width/height."""
+        lib = load_library()
+        keep = {}
+        d = SceneDesc()
+        for key, dt in (("spheres", SPHERE), ("vertices", np.float32), ("triangles", TRIANGLE),
+                        ("materials", MATERIAL), ("nodes", BVH_NODE), ("prim_order", np.int32), ("lights", LIGHT)):
+            a = arrays.get(key)
+            a = np.ascontiguousarray(a if a is not None else np.zeros(0, dt), dtype=dt)
+            if key == "vertices":
+                a = a.reshape(-1, 3)
+            keep[key] = a
+            setattr(d, key, a.ctypes.data if a.size else None)
+            setattr(d, "n_" + key, int(a.shape[0]))
+        d.env = (ctypes.c_float * 3)(*arrays["env"])
+        d.cam_position = (ctypes.c_float * 3)(*arrays["cam_position"])
+        d.cam_look_at = (ctypes.c_float * 3)(*arrays["cam_look_at"])
+        d.cam_up = (ctypes.c_float * 3)(*arrays["cam_up"])
+        d.cam_vfov_deg = float(arrays["cam_vfov_deg"])
+        d.width, d.height = int(arrays["width"]), int(arrays["height"])
+        h = ctypes.c_void_p()
+        _check(lib.wfb_scene_create(ctypes.byref(d), finalize_bins, ctypes.byref(h)))
+        return cls(h.value)
+
+    def info(self) -> SceneInfo:
+        inf = SceneInfo()
+        _check(load_library().wfb_scene_info_get(self._h, ctypes.byref(inf)))
+        return inf
+
+    def export(self) -> dict:
+        """Finalized host arrays in the reference layouts + env, camera and resolution."""
+        inf = self.info()
+        out = {
+            "spheres": np.zeros(inf.n_spheres, SPHERE),
+            "vertices": np.zeros((inf.n_vertices, 3), np.float32),
+            "triangles": np.zeros(inf.n_triangles, TRIANGLE),
+            "materials": np.zeros(inf.n_materials, MATERIAL),
+            "nodes": np.zeros(inf.n_nodes, BVH_NODE),
+            "prim_order": np.zeros(inf.n_prim_order, np.int32),
+            "lights": np.zeros(inf.n_lights, LIGHT),
+        }
+        _check(load_library().wfb_scene_export(self._h, *[_ptr(out[k]) for k in (
+            "spheres", "vertices", "triangles", "materials", "nodes", "prim_order", "lights")]))
+        out.update(env=list(inf.env), cam_position=list(inf.cam_position), cam_look_at=list(inf.cam_look_at),
+                   cam_up=list(inf.cam_up), cam_vfov_deg=inf.cam_vfov_deg, width=inf.width, height=inf.height)
+        return out
+
+    def hash(self) -> int:
+        return int(load_library().wfb_scene_hash(self._h))
+
+    def validate_bvh(self) -> str:
+        buf = ctypes.create_string_buffer(256)
+        _check(load_library().wfb_scene_validate_bvh(self._h, buf, 256))
+        return buf.value.decode()
+
+    def device_bytes(self) -> int:
+        return int(load_library().wfb_scene_device_bytes(self._h))
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            load_library().wfb_scene_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuRenderer:
+    """wf::GpuRenderer (WVM/include/wf/renderer.hpp:44-67) on this engine's sm_100a kernels."""
+
+    def __init__(self, scene: Scene, mode: int = MEGAKERNEL):
+        self._scene = scene  # keeps the scene handle alive
+        h = ctypes.c_void_p()
+        _check(load_library().wfb_renderer_create(scene.handle, int(mode), ctypes.byref(h)))
+        self._h = h
+        self.mode = mode
+
+    @property
+    def width(self) -> int:
+        return int(load_library().wfb_renderer_width(self._h))
+
+    @property
+    def height(self) -> int:
+        return int(load_library().wfb_renderer_height(self._h))
+
+    def set_camera(self, position, look_at, up, vfov_deg: float, width: int, height: int) -> None:
+        f3 = ctypes.c_float * 3
+        _check(load_library().wfb_renderer_set_camera(self._h, f3(*position), f3(*look_at), f3(*up),
+                                                       float(vfov_deg), int(width), int(height)))
+
+    def reset(self) -> None:
+        _check(load_library().wfb_renderer_reset(self._h))
+
+    def run_passes(self, first_sample: int, count: int, params: RenderParams, stats: RenderStats | None = None):
+        cs = _CRenderStats()
+        _check(load_library().wfb_renderer_run_passes(self._h, first_sample, count, ctypes.byref(params._c()),
+                                                       ctypes.byref(cs)))
+        st = RenderStats._from_c(cs)
+        if stats is not None:
+            stats.__dict__.update(st.__dict__)
+        return st
+
+    def download(self, spp_done: int) -> RenderResult:
+        w, h = self.width, self.height
+        rgb = np.empty((h, w, 3), np.float32)
+        var = np.empty((h, w), np.float32)
+        _check(load_library().wfb_renderer_download(self._h, spp_done, _ptr(rgb), _ptr(var)))
+        return RenderResult(w, h, spp_done, rgb, var)
+
+    def download_mean(self, spp_done: int) -> np.ndarray:
+        rgb = np.empty((self.height, self.width, 3), np.float32)
+        _check(load_library().wfb_renderer_download_mean(self._h, spp_done, _ptr(rgb)))
+        return rgb
+
+    def download_sums(self):
+        w, h = self.width, self.height
+        rgb = np.empty((h, w, 3), np.float32)
+        lum = np.empty((h, w), np.float32)
+        lum2 = np.empty((h, w), np.float32)
+        _check(load_library().wfb_renderer_download_sums(self._h, _ptr(rgb), _ptr(lum), _ptr(lum2)))
+        return rgb, lum, lum2
+
+    def render(self, params: RenderParams, stats: RenderStats | None = None) -> RenderResult:
+        w, h = self.width, self.height
+        rgb = np.empty((h, w, 3), np.float32)
+        var = np.empty((h, w), np.float32)
+        cs = _CRenderStats()
+        _check(load_library().wfb_renderer_render(self._h, ctypes.byref(params._c()), ctypes.byref(cs),
+                                                   _ptr(rgb), _ptr(var)))
+        if stats is not None:
+            stats.__dict__.update(RenderStats._from_c(cs).__dict__)
+        return RenderResult(w, h, params.spp, rgb, var)
+
+    def device_bytes(self) -> int:
+        return int(load_library().wfb_renderer_device_bytes(self._h))
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            load_library().wfb_renderer_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def compare_results(a: RenderResult, b: RenderResult) -> dict:
+    """wf::compare_results (WVM/src/film.cpp:45-113): max_abs_rel, mean_rel, frac_within_3se, nonfinite."""
+    if a.width != b.width or a.height != b.height:
+        raise ValueError("compare_results: image dimensions mismatch")
+    ra, rb = a.rgb.reshape(-1, 3), b.rgb.reshape(-1, 3)
+    n = ra.shape[0]
+    w = np.array([0.2126, 0.7152, 0.0722], np.float32)
+    la = (np.float32(w[0]) * ra[:, 0] + np.float32(w[1]) * ra[:, 1]) + np.float32(w[2]) * ra[:, 2]
+    lb = (np.float32(w[0]) * rb[:, 0] + np.float32(w[1]) * rb[:, 1]) + np.float32(w[2]) * rb[:, 2]
+    fin = np.isfinite(ra) & np.isfinite(rb)
+    nonfinite = int((~np.isfinite(ra)).sum() + (~np.isfinite(rb)).sum())
+    denom = np.maximum(np.maximum(np.abs(ra), np.abs(rb)), np.float32(1e-6))
+    rel = np.where(fin, np.abs(ra - rb) / denom, 0.0)
+    sea = np.sqrt(a.lum_var.reshape(-1) / np.float32(a.spp))
+    seb = np.sqrt(b.lum_var.reshape(-1) / np.float32(b.spp))
+    within = np.abs(la - lb) <= np.float32(3.0) * np.sqrt(sea * sea + seb * seb)
+    within &= np.isfinite(la) & np.isfinite(lb)
+    mean_a, mean_b = float(la.astype(np.float64).mean()), float(lb.astype(np.float64).mean())
+    mean_rel = abs(mean_a - mean_b) / mean_a if mean_a > 1e-12 else abs(mean_a - mean_b)
+    return {"max_abs_rel": float(rel.max()) if n else 0.0, "mean_rel": mean_rel,
+            "frac_within_3se": float(within.mean()) if n else 0.0, "nonfinite": nonfinite}

@@ -1,0 +1,301 @@
+// extern "C" boundary (include/wfb200.h): status codes instead of exceptions, opaque handles.
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <mutex>
+#include <string>
+#include "engine.hpp"
+#include "scene_gen.hpp"
+#include "../../include/wfb200.h"
+
+struct wfb_scene {
+    wf::Scene host;
+    std::shared_ptr<wfb::ResidentScene> resident;  // uploaded on first use
+    std::mutex mu;
+    std::shared_ptr<wfb::ResidentScene> get_resident() {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!resident) resident = wfb::upload_scene(host);
+        return resident;
+    }
+};
+
+struct wfb_renderer {
+    std::unique_ptr<wfb::Renderer> r;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        g_last_error.clear();
+        f();
+        return WFB_OK;
+    } catch (const wfb::Error& e) {
+        return fail(e.status, e.what());
+    } catch (const std::invalid_argument& e) {
+        return fail(WFB_ERR_INVALID_ARGUMENT, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(WFB_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(WFB_ERR_INVALID_ARGUMENT, e.what());
+    } catch (...) {
+        return fail(WFB_ERR_INTERNAL, "unknown exception");
+    }
+}
+
+wfb::PassParams pass_params(const wfb_render_params* p, int first, int count) {
+    wfb::PassParams q;
+    q.first_sample = first;
+    q.sample_count = count;
+    q.seed = p->seed;
+    q.max_depth = p->max_depth;
+    q.count_rays = p->count_rays != 0;
+    q.stage_timing = p->stage_timing != 0;
+    q.queue_capacity = p->queue_capacity;
+    return q;
+}
+
+void to_c_stats(const wf::RenderStats& s, wfb_render_stats* out) {
+    out->render_ms = s.render_ms;
+    out->total_ms = s.total_ms;
+    out->extension_rays = s.extension_rays;
+    out->shadow_rays = s.shadow_rays;
+    for (int i = 0; i < 5; ++i) out->queue_high_water[i] = s.queue_high_water[i];
+    out->queue_overflows = s.queue_overflows;
+    out->invalid_hits = s.invalid_hits;
+    out->peak_vram_bytes = s.peak_vram_bytes;
+    const double st[8] = {s.stages.extend, s.stages.classify, s.stages.shade_lambert, s.stages.shade_metal,
+                          s.stages.shade_dielectric, s.stages.shadow, s.stages.compact, s.stages.other};
+    for (int i = 0; i < 8; ++i) out->stage_ms[i] = st[i];
+}
+
+void need(bool ok, const char* msg) {
+    if (!ok) throw wfb::Error(WFB_ERR_INVALID_ARGUMENT, msg);
+}
+
+}  // namespace
+
+extern "C" {
+
+int wfb_abi_version(void) { return WFB_ABI_VERSION; }
+
+const char* wfb_last_error(void) { return g_last_error.c_str(); }
+
+int wfb_device_name(char* buf, int len) {
+    return guarded([&] {
+        need(buf && len > 0, "null buffer");
+        int dev = 0;
+        wfb::cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cudaDeviceProp prop;
+        wfb::cuda_check(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+        std::strncpy(buf, prop.name, (size_t)len - 1);
+        buf[len - 1] = '\0';
+    });
+}
+
+int wfb_scene_create(const wfb_scene_desc* d, int finalize_bins, wfb_scene_t* out) {
+    return guarded([&] {
+        need(d && out, "null argument");
+        need(d->n_spheres >= 0 && d->n_vertices >= 0 && d->n_triangles >= 0 && d->n_materials >= 0 &&
+                 d->n_nodes >= 0 && d->n_prim_order >= 0 && d->n_lights >= 0,
+             "negative array size");
+        auto s = std::make_unique<wfb_scene>();
+        wf::Scene& h = s->host;
+        auto copy = [](auto& vec, const void* src, int n) {
+            vec.resize((size_t)n);
+            if (n) std::memcpy(vec.data(), src, sizeof(vec[0]) * (size_t)n);
+        };
+        need((d->n_spheres == 0 || d->spheres) && (d->n_vertices == 0 || d->vertices) &&
+                 (d->n_triangles == 0 || d->triangles) && (d->n_materials == 0 || d->materials) &&
+                 (d->n_nodes == 0 || d->nodes) && (d->n_prim_order == 0 || d->prim_order) &&
+                 (d->n_lights == 0 || d->lights),
+             "null array with a nonzero size");
+        copy(h.spheres, d->spheres, d->n_spheres);
+        copy(h.vertices, d->vertices, d->n_vertices);
+        copy(h.triangles, d->triangles, d->n_triangles);
+        copy(h.materials, d->materials, d->n_materials);
+        copy(h.nodes, d->nodes, d->n_nodes);
+        copy(h.prim_order, d->prim_order, d->n_prim_order);
+        copy(h.lights, d->lights, d->n_lights);
+        h.env = wf::Vec3{d->env[0], d->env[1], d->env[2]};
+        h.camera.position = wf::Vec3{d->cam_position[0], d->cam_position[1], d->cam_position[2]};
+        h.camera.look_at = wf::Vec3{d->cam_look_at[0], d->cam_look_at[1], d->cam_look_at[2]};
+        h.camera.up = wf::Vec3{d->cam_up[0], d->cam_up[1], d->cam_up[2]};
+        h.camera.vfov_deg = d->cam_vfov_deg;
+        need(d->width > 0 && d->height > 0, "resolution must be positive");
+        h.width = d->width;
+        h.height = d->height;
+        if (finalize_bins > 0) wf::finalize_scene_bins(h, finalize_bins);
+        *out = s.release();
+    });
+}
+
+int wfb_scene_generate(const char* name, int width, int height, uint32_t seed, int sah_bins,
+                       wfb_scene_t* out) {
+    return guarded([&] {
+        need(name && out, "null argument");
+        auto s = std::make_unique<wfb_scene>();
+        s->host = wfb::make_config_scene(name, width, height, seed, sah_bins > 0 ? sah_bins : 16);
+        *out = s.release();
+    });
+}
+
+int wfb_scene_info_get(wfb_scene_t s, wfb_scene_info* info) {
+    return guarded([&] {
+        need(s && info, "null argument");
+        const wf::Scene& h = s->host;
+        info->n_spheres = (int)h.spheres.size();
+        info->n_vertices = (int)h.vertices.size();
+        info->n_triangles = (int)h.triangles.size();
+        info->n_materials = (int)h.materials.size();
+        info->n_nodes = (int)h.nodes.size();
+        info->n_prim_order = (int)h.prim_order.size();
+        info->n_lights = (int)h.lights.size();
+        info->width = h.width;
+        info->height = h.height;
+        const float env[3] = {h.env.x, h.env.y, h.env.z};
+        std::memcpy(info->env, env, sizeof(env));
+        const float pos[3] = {h.camera.position.x, h.camera.position.y, h.camera.position.z};
+        const float at[3] = {h.camera.look_at.x, h.camera.look_at.y, h.camera.look_at.z};
+        const float up[3] = {h.camera.up.x, h.camera.up.y, h.camera.up.z};
+        std::memcpy(info->cam_position, pos, sizeof(pos));
+        std::memcpy(info->cam_look_at, at, sizeof(at));
+        std::memcpy(info->cam_up, up, sizeof(up));
+        info->cam_vfov_deg = h.camera.vfov_deg;
+    });
+}
+
+int wfb_scene_export(wfb_scene_t s, void* spheres, float* vertices, int* triangles, void* materials,
+                     void* nodes, int* prim_order, void* lights) {
+    return guarded([&] {
+        need(s != nullptr, "null scene");
+        const wf::Scene& h = s->host;
+        auto put = [](void* dst, const auto& vec) {
+            if (dst && !vec.empty()) std::memcpy(dst, vec.data(), sizeof(vec[0]) * vec.size());
+        };
+        put(spheres, h.spheres);
+        put(vertices, h.vertices);
+        put(triangles, h.triangles);
+        put(materials, h.materials);
+        put(nodes, h.nodes);
+        put(prim_order, h.prim_order);
+        put(lights, h.lights);
+    });
+}
+
+uint64_t wfb_scene_hash(wfb_scene_t s) { return s ? wf::scene_hash(s->host) : 0; }
+
+int wfb_scene_validate_bvh(wfb_scene_t s, char* msg, int len) {
+    return guarded([&] {
+        need(s && msg && len > 0, "null argument");
+        const std::string m = wf::validate_bvh(s->host);
+        std::strncpy(msg, m.c_str(), (size_t)len - 1);
+        msg[len - 1] = '\0';
+    });
+}
+
+int wfb_scene_destroy(wfb_scene_t s) {
+    delete s;
+    return WFB_OK;
+}
+
+uint64_t wfb_scene_device_bytes(wfb_scene_t s) {
+    if (!s) return 0;
+    std::lock_guard<std::mutex> lock(s->mu);
+    return s->resident ? s->resident->bytes : 0;
+}
+
+int wfb_renderer_create(wfb_scene_t s, int mode, wfb_renderer_t* out) {
+    return guarded([&] {
+        need(s && out, "null argument");
+        need(mode == WFB_MODE_MEGAKERNEL || mode == WFB_MODE_WAVEFRONT, "unknown mode");
+        if (s->host.nodes.empty()) throw wfb::Error(WFB_ERR_NOT_FINALIZED, "Scene not finalized (no BVH nodes)");
+        auto r = std::make_unique<wfb_renderer>();
+        r->r = std::make_unique<wfb::Renderer>(s->get_resident(),
+                                               mode == WFB_MODE_WAVEFRONT ? wf::GpuMode::Wavefront : wf::GpuMode::Megakernel);
+        *out = r.release();
+    });
+}
+
+int wfb_renderer_set_camera(wfb_renderer_t r, const float position[3], const float look_at[3],
+                            const float up[3], float vfov_deg, int width, int height) {
+    return guarded([&] {
+        need(r && position && look_at && up, "null argument");
+        wf::Camera c;
+        c.position = wf::Vec3{position[0], position[1], position[2]};
+        c.look_at = wf::Vec3{look_at[0], look_at[1], look_at[2]};
+        c.up = wf::Vec3{up[0], up[1], up[2]};
+        c.vfov_deg = vfov_deg;
+        r->r->set_camera(c, width, height);
+    });
+}
+
+int wfb_renderer_reset(wfb_renderer_t r) {
+    return guarded([&] {
+        need(r != nullptr, "null renderer");
+        r->r->reset();
+    });
+}
+
+int wfb_renderer_run_passes(wfb_renderer_t r, int first_sample, int count, const wfb_render_params* p,
+                            wfb_render_stats* stats) {
+    return guarded([&] {
+        need(r && p, "null argument");
+        wf::RenderStats st{};
+        r->r->run_passes(pass_params(p, first_sample, count), &st);
+        if (stats) to_c_stats(st, stats);
+    });
+}
+
+int wfb_renderer_download(wfb_renderer_t r, int spp_done, float* rgb, float* lum_var) {
+    return guarded([&] {
+        need(r != nullptr, "null renderer");
+        r->r->download(spp_done, rgb, lum_var);
+    });
+}
+
+int wfb_renderer_download_mean(wfb_renderer_t r, int spp_done, float* rgb) {
+    return guarded([&] {
+        need(r && rgb, "null argument");
+        r->r->download_mean(spp_done, rgb);
+    });
+}
+
+int wfb_renderer_download_sums(wfb_renderer_t r, float* rgb_sum, float* lum_sum, float* lum2_sum) {
+    return guarded([&] {
+        need(r != nullptr, "null renderer");
+        r->r->download_sums(rgb_sum, lum_sum, lum2_sum);
+    });
+}
+
+int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render_stats* stats, float* rgb,
+                        float* lum_var) {
+    return guarded([&] {
+        need(r && p, "null argument");
+        need(p->spp > 0, "spp must be positive");
+        r->r->reset();
+        wf::RenderStats st{};
+        r->r->run_passes(pass_params(p, 0, p->spp), &st);
+        r->r->download(p->spp, rgb, lum_var);
+        if (stats) to_c_stats(st, stats);
+    });
+}
+
+uint64_t wfb_renderer_device_bytes(wfb_renderer_t r) { return r ? r->r->device_bytes() : 0; }
+int wfb_renderer_width(wfb_renderer_t r) { return r ? r->r->width() : 0; }
+int wfb_renderer_height(wfb_renderer_t r) { return r ? r->r->height() : 0; }
+
+int wfb_renderer_destroy(wfb_renderer_t r) {
+    delete r;
+    return WFB_OK;
+}
+
+}  // extern "C"

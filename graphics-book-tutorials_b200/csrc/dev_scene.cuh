@@ -1,0 +1,211 @@
+// Device-resident scene in this engine's packed layout, and the traversal over it.
+//
+// Layout (all arrays 16-byte aligned, read through the read-only path with 16-byte loads):
+//   nodes     2 x float4 per BVH node, preorder (same order and skip links as wf::BvhNode):
+//               {lo.x, lo.y, lo.z, skip}  {hi.x, hi.y, hi.z, leaf}
+//             leaf = -1 for an internal node, else prim_start * 16 + prim_count (count 1..15).
+//             32 B per node instead of 48 B: a box test is exactly two 16-byte loads.
+//   prims     3 x float4 per prim_order entry (leaf primitives are contiguous):
+//               triangle {p0, id} {e1, 0} {e2, 0} with e1 = p1 - p0, e2 = p2 - p0
+//               sphere   {centre, id} {radius, 0, 0, 0} {0}
+//             one dependent load level (node -> record) instead of three
+//             (node -> prim_order -> triangle -> 3 vertices).
+//   spheres   2 x float4 per sphere (wf::Sphere bytes)
+//   tri_shade 1 x float4 per triangle {normalize(cross(e1, e2)), material}
+//   tri_area  1 float per triangle: 0.5 * length(cross(e1, e2))
+//   materials 3 x float4 per material (wf::Material bytes)
+//   lights    4 x float4 per light {a, prim} {b, area} {c, material} {n, radius}
+// Every precomputed float is produced on the host by the same IEEE operations the reference
+// evaluates per ray (WVM/include/wf/bvh.hpp:44-61, WVM/include/wf/path_core.hpp:44-53,84-101,
+// 124-131), so the device results are bit-identical to the reference's.
+#pragma once
+#include <cuda_runtime.h>
+#include "wf/path_core.hpp"
+
+namespace wfb {
+
+struct DevScene {
+    const float4* nodes;
+    const float4* prims;
+    const float4* spheres;
+    const float4* tri_shade;
+    const float* tri_area;
+    const float4* materials;
+    const float4* lights;
+    int n_spheres, n_triangles, n_materials, n_nodes, n_lights;
+    wf::Vec3 env;
+    wf::CameraRig camera;
+    int width, height;
+};
+
+constexpr int kLeafCountBits = 4;
+constexpr int kLeafCountMask = (1 << kLeafCountBits) - 1;
+constexpr int kMaxLeafPrims = kLeafCountMask;
+constexpr long long kMaxLeafStart = (1LL << (31 - kLeafCountBits)) - 1;
+
+template <class T>
+WF_HD T ro_load(const T* p) {
+#if defined(__CUDA_ARCH__)
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
+WF_HD int f2i(float f) {
+#if defined(__CUDA_ARCH__)
+    return __float_as_int(f);
+#else
+    int i;
+    __builtin_memcpy(&i, &f, 4);
+    return i;
+#endif
+}
+
+// ---- accessors used by the estimator templates (wf/path_core.hpp) ----
+WF_HD wf::Sphere load_sphere(const DevScene& s, int i) {
+    const float4 a = ro_load(&s.spheres[2 * i]);
+    const float4 b = ro_load(&s.spheres[2 * i + 1]);
+    wf::Sphere sp;
+    sp.center = wf::Vec3{a.x, a.y, a.z};
+    sp.radius = a.w;
+    sp.material = f2i(b.x);
+    sp.pad[0] = sp.pad[1] = sp.pad[2] = 0;
+    return sp;
+}
+WF_HD wf::Material load_material(const DevScene& s, int m) {
+    const float4 a = ro_load(&s.materials[3 * m]);
+    const float4 b = ro_load(&s.materials[3 * m + 1]);
+    const float4 c = ro_load(&s.materials[3 * m + 2]);
+    wf::Material mat;
+    mat.type = f2i(a.x);
+    mat.ior = a.y;
+    mat.pad0 = a.z;
+    mat.pad1 = a.w;
+    mat.albedo = wf::Vec3{b.x, b.y, b.z};
+    mat.pad2 = b.w;
+    mat.emission = wf::Vec3{c.x, c.y, c.z};
+    mat.pad3 = c.w;
+    return mat;
+}
+WF_HD int tri_material(const DevScene& s, int t) { return f2i(ro_load(&s.tri_shade[t]).w); }
+WF_HD wf::Vec3 tri_normal(const DevScene& s, int t) {
+    const float4 a = ro_load(&s.tri_shade[t]);
+    return wf::Vec3{a.x, a.y, a.z};
+}
+WF_HD float prim_area(const DevScene& s, int prim) {
+    if (prim < s.n_spheres) {
+        const float r = ro_load(&s.spheres[2 * prim]).w;
+        return 4.0f * wf::kPi * r * r;
+    }
+    return ro_load(&s.tri_area[prim - s.n_spheres]);
+}
+WF_HD wf::LightGeom load_light(const DevScene& s, int idx) {
+    const float4 a = ro_load(&s.lights[4 * idx]);
+    const float4 b = ro_load(&s.lights[4 * idx + 1]);
+    const float4 c = ro_load(&s.lights[4 * idx + 2]);
+    const float4 d = ro_load(&s.lights[4 * idx + 3]);
+    wf::LightGeom g;
+    g.prim = f2i(a.w);
+    g.is_sphere = g.prim < s.n_spheres ? 1 : 0;
+    g.a = wf::Vec3{a.x, a.y, a.z};
+    g.b = wf::Vec3{b.x, b.y, b.z};
+    g.area = b.w;
+    g.c = wf::Vec3{c.x, c.y, c.z};
+    g.material = f2i(c.w);
+    g.n = wf::Vec3{d.x, d.y, d.z};
+    g.radius = d.w;
+    return g;
+}
+
+#if defined(__CUDACC__)
+// Stackless preorder skip-link traversal over the packed nodes: the same visiting order, the
+// same box and primitive arithmetic and the same strictly-nearer replacement rule as
+// wf::intersect (WVM/include/wf/bvh.hpp:91-116), so hit ids, t, u and v are bit-identical.
+// Returns true on a hit. `tests` (optional) accumulates node visits for instrumentation.
+__device__ __forceinline__ bool intersect_dev(const DevScene& s, wf::Ray r, wf::HitRecord* h,
+                                              bool anyhit) {
+    h->t = r.tmax;
+    h->prim = -1;
+    h->u = 0.0f;
+    h->v = 0.0f;
+    const wf::Vec3 inv_d{1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z};
+    int n = 0;
+    while (n >= 0 && n < s.n_nodes) {
+        const float4 a = __ldg(&s.nodes[2 * n]);
+        const float4 b = __ldg(&s.nodes[2 * n + 1]);
+        const int skip = __float_as_int(a.w);
+        if (!wf::hit_box(wf::Vec3{a.x, a.y, a.z}, wf::Vec3{b.x, b.y, b.z}, r.o, inv_d, r.tmin,
+                         r.tmax)) {
+            n = skip;
+            continue;
+        }
+        const int leaf = __float_as_int(b.w);
+        if (leaf < 0) {
+            n = n + 1;
+            continue;
+        }
+        const int start = leaf >> kLeafCountBits;
+        const int count = leaf & kLeafCountMask;
+        const float4* rec = s.prims + 3 * start;
+        for (int i = 0; i < count; ++i, rec += 3) {
+            const float4 q0 = __ldg(rec);
+            const float4 q1 = __ldg(rec + 1);
+            const int p = __float_as_int(q0.w);
+            float t, u = 0.0f, v = 0.0f;
+            bool hit;
+            if (p < s.n_spheres) {
+                hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
+            } else {
+                const float4 q2 = __ldg(rec + 2);
+                hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
+                                            wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
+            }
+            if (hit) {
+                r.tmax = t;
+                h->t = t;
+                h->prim = p;
+                h->u = u;
+                h->v = v;
+                if (anyhit) return true;
+            }
+        }
+        n = skip;
+    }
+    return h->prim >= 0;
+}
+
+// Validity check applied after every closest-hit query (WVM/src/gpu/engine.cuh:44-48).
+__device__ __forceinline__ bool hit_is_valid(const DevScene& s, const wf::HitRecord& h) {
+    if (h.prim < 0) return true;
+    const int total = s.n_spheres + s.n_triangles;
+    return h.prim < total && wf::is_finite1(h.t) && h.t > 0.0f;
+}
+
+#endif  // __CUDACC__
+
+// Per-pixel running sums (WVM/src/gpu/engine.cuh:18-32): rgb[3P], lum[P], lum2[P]. A pixel has one
+// writer at a time and samples are added in ascending sample order, never with atomics.
+struct DevFilm {
+    float* rgb;
+    float* lum;
+    float* lum2;
+    int pixels;
+};
+
+// Counters shared by every engine (layout is internal to this library).
+struct DevCounters {
+    unsigned long long extension_rays;
+    unsigned long long shadow_rays;
+    unsigned int invalid_hits;
+    unsigned int overflows;
+    unsigned int high_water[5];
+    unsigned int error;  // nonzero: a bounded wait gave up (see kErr* codes)
+};
+
+enum : unsigned int {
+    kErrNone = 0,
+    kErrSpinTimeout = 1,  // a grid-wide wait or a scan lookback exceeded its poll limit
+};
+
+}  // namespace wfb

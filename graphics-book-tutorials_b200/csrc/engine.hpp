@@ -1,0 +1,100 @@
+// Engine internals shared by the kernels' host launchers, the renderer and the C ABI.
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "dev_scene.cuh"
+#include "wf/renderer.hpp"
+#include "wf/scene.hpp"
+
+namespace wfb {
+
+// Error carrying one of the C ABI status codes (include/wfb200.h).
+struct Error : std::runtime_error {
+    int status;
+    Error(int st, const std::string& msg) : std::runtime_error(msg), status(st) {}
+};
+
+void cuda_check(cudaError_t e, const char* what);  // throws Error(WFB_ERR_CUDA or OOM)
+
+// Scene uploaded once in the packed device layout; shared (reference-counted) by every renderer
+// and batch job that draws it, so a BVH stays resident across renders.
+struct ResidentScene {
+    wf::Scene host;  // finalized host copy (source of truth for export, hashing, cameras)
+    DevScene dev{};  // device pointers into `arena`; camera/resolution are the host defaults
+    void* arena = nullptr;
+    uint64_t bytes = 0;
+    int device = -1;
+    ~ResidentScene();
+};
+
+// Validates and repacks a finalized scene into the device layout (see dev_scene.cuh).
+std::shared_ptr<ResidentScene> upload_scene(wf::Scene host);
+
+// Same scene view with another camera / resolution (batch jobs and orbit cameras).
+DevScene with_camera(const DevScene& s, const wf::Camera& cam, int width, int height);
+
+// Per-call render controls (mirror of wf::RenderParams without the CPU-only fields).
+struct PassParams {
+    int first_sample = 0;
+    int sample_count = 0;
+    uint32_t seed = 1234;
+    int max_depth = 8;
+    bool count_rays = false;
+    bool stage_timing = false;
+    int queue_capacity = 0;
+};
+
+// ---- megakernel (megakernel.cu) ----
+struct MegakernelConfig {
+    int block = 128;     // threads per block
+    int blocks_per_sm = 0;  // 0: maximum resident
+};
+// Renders samples [first, first + count) of every pixel into `film` (adding to its sums).
+void launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters,
+                       unsigned int* work_counter, const PassParams& p,
+                       const MegakernelConfig& cfg, cudaStream_t stream);
+
+// ---- GPU renderer (renderer.cu): one scene, one camera, one film ----
+class Renderer {
+public:
+    Renderer(std::shared_ptr<ResidentScene> scene, wf::GpuMode mode);
+    ~Renderer();
+    Renderer(const Renderer&) = delete;
+    Renderer& operator=(const Renderer&) = delete;
+
+    void set_camera(const wf::Camera& cam, int width, int height);
+    void reset();
+    void run_passes(const PassParams& p, wf::RenderStats* stats);
+    // Reference download convention (WVM/src/gpu/gpu_renderer.cu:306-341).
+    void download(int spp_done, float* rgb, float* lum_var);
+    void download_mean(int spp_done, float* rgb);
+    void download_sums(float* rgb_sum, float* lum_sum, float* lum2_sum);
+    uint64_t device_bytes() const;
+    int width() const { return width_; }
+    int height() const { return height_; }
+    int pixels() const { return width_ * height_; }
+    wf::GpuMode mode() const { return mode_; }
+    void set_megakernel_config(const MegakernelConfig& c) { mk_cfg_ = c; }
+
+private:
+    void alloc_film();
+    void free_film();
+    std::shared_ptr<ResidentScene> scene_;
+    DevScene view_{};
+    wf::GpuMode mode_;
+    int width_ = 0, height_ = 0;
+    DevFilm film_{};
+    DevCounters* counters_ = nullptr;
+    unsigned int* work_ = nullptr;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    MegakernelConfig mk_cfg_{};
+    struct Wavefront;
+    std::unique_ptr<Wavefront> wf_;
+};
+
+}  // namespace wfb

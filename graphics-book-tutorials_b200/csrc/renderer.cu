@@ -1,0 +1,145 @@
+// GPU renderer: one resident scene, one camera, one film (the wf::GpuRenderer contract,
+// WVM/src/gpu/gpu_renderer.cu:100-377) on this engine's kernels.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+#include "engine.hpp"
+#include "wavefront.hpp"
+#include "../../include/wfb200.h"
+
+namespace wfb {
+
+struct Renderer::Wavefront {
+    WavefrontEngine engine;
+    explicit Wavefront(int pixels) : engine(pixels) {}
+};
+
+Renderer::Renderer(std::shared_ptr<ResidentScene> scene, wf::GpuMode mode)
+    : scene_(std::move(scene)), mode_(mode) {
+    if (!scene_) throw Error(WFB_ERR_INVALID_ARGUMENT, "null scene");
+    view_ = scene_->dev;
+    width_ = view_.width;
+    height_ = view_.height;
+    cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaEventCreate(&ev0_), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&ev1_), "cudaEventCreate");
+    cuda_check(cudaMalloc(&counters_, sizeof(DevCounters)), "cudaMalloc counters");
+    cuda_check(cudaMalloc(&work_, 256), "cudaMalloc work counter");
+    alloc_film();
+}
+
+Renderer::~Renderer() {
+    free_film();
+    wf_.reset();
+    if (counters_) cudaFree(counters_);
+    if (work_) cudaFree(work_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Renderer::alloc_film() {
+    const size_t p = (size_t)width_ * height_;
+    float* base = nullptr;
+    cuda_check(cudaMalloc(&base, 5 * p * sizeof(float)), "cudaMalloc film");
+    film_.rgb = base;
+    film_.lum = base + 3 * p;
+    film_.lum2 = base + 4 * p;
+    film_.pixels = (int)p;
+    cuda_check(cudaMemset(base, 0, 5 * p * sizeof(float)), "cudaMemset film");
+    if (mode_ == wf::GpuMode::Wavefront) wf_ = std::make_unique<Wavefront>((int)p);
+}
+
+void Renderer::free_film() {
+    if (film_.rgb) cudaFree(film_.rgb);
+    film_ = DevFilm{};
+    wf_.reset();
+}
+
+void Renderer::set_camera(const wf::Camera& cam, int width, int height) {
+    if (width <= 0 || height <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "resolution must be positive");
+    cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    view_ = with_camera(scene_->dev, cam, width, height);
+    if (width != width_ || height != height_) {
+        free_film();
+        width_ = width;
+        height_ = height;
+        alloc_film();
+    } else {
+        reset();
+    }
+}
+
+void Renderer::reset() {
+    cuda_check(cudaMemsetAsync(film_.rgb, 0, 5 * (size_t)pixels() * sizeof(float), stream_), "cudaMemset film");
+    cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+}
+
+void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
+    if (p.sample_count < 0 || p.first_sample < 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "negative sample range");
+    if (p.max_depth < 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "max_depth must be >= 0");
+    cuda_check(cudaMemsetAsync(counters_, 0, sizeof(DevCounters), stream_), "zero counters");
+    cuda_check(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    if (mode_ == wf::GpuMode::Megakernel) {
+        launch_megakernel(view_, film_, counters_, work_, p, mk_cfg_, stream_);
+    } else {
+        wf_->engine.run(view_, film_, counters_, p, stats ? &stats->stages : nullptr, stream_);
+    }
+    cuda_check(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
+    cuda_check(cudaEventSynchronize(ev1_), "render");
+    DevCounters c{};
+    cuda_check(cudaMemcpy(&c, counters_, sizeof(c), cudaMemcpyDeviceToHost), "download counters");
+    if (c.error != kErrNone)
+        throw Error(WFB_ERR_DEVICE_WAIT, "a bounded device-side wait gave up; the render is incomplete");
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev0_, ev1_);
+        stats->render_ms = ms;
+        stats->extension_rays += c.extension_rays;
+        stats->shadow_rays += c.shadow_rays;
+        stats->invalid_hits += c.invalid_hits;
+        stats->queue_overflows += c.overflows;
+        for (int i = 0; i < 5; ++i)
+            stats->queue_high_water[i] = std::max(stats->queue_high_water[i], (long long)c.high_water[i]);
+        stats->peak_vram_bytes = device_bytes();
+    }
+}
+
+void Renderer::download_sums(float* rgb_sum, float* lum_sum, float* lum2_sum) {
+    const size_t p = (size_t)pixels();
+    cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    if (rgb_sum) cuda_check(cudaMemcpy(rgb_sum, film_.rgb, 3 * p * sizeof(float), cudaMemcpyDeviceToHost), "download rgb");
+    if (lum_sum) cuda_check(cudaMemcpy(lum_sum, film_.lum, p * sizeof(float), cudaMemcpyDeviceToHost), "download lum");
+    if (lum2_sum) cuda_check(cudaMemcpy(lum2_sum, film_.lum2, p * sizeof(float), cudaMemcpyDeviceToHost), "download lum2");
+}
+
+void Renderer::download(int spp_done, float* rgb, float* lum_var) {
+    if (spp_done <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "spp_done must be positive");
+    const size_t p = (size_t)pixels();
+    std::vector<float> lum, lum2;
+    if (lum_var) {
+        lum.resize(p);
+        lum2.resize(p);
+    }
+    download_sums(rgb, lum_var ? lum.data() : nullptr, lum_var ? lum2.data() : nullptr);
+    const float inv = 1.0f / (float)spp_done;
+    if (rgb)
+        for (size_t i = 0; i < 3 * p; ++i) rgb[i] *= inv;
+    if (lum_var) {
+        for (size_t i = 0; i < p; ++i) {
+            const double m = (double)lum[i] / (double)spp_done;
+            const double m2 = (double)lum2[i] / (double)spp_done;
+            lum_var[i] = (float)std::max(0.0, m2 - m * m);
+        }
+    }
+}
+
+void Renderer::download_mean(int spp_done, float* rgb) { download(spp_done, rgb, nullptr); }
+
+uint64_t Renderer::device_bytes() const {
+    uint64_t b = scene_->bytes + 5ull * pixels() * sizeof(float) + sizeof(DevCounters);
+    if (wf_) b += wf_->engine.bytes();
+    return b;
+}
+
+}  // namespace wfb

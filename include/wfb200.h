@@ -1,0 +1,156 @@
+/*
+ * wfb200 -- C ABI of the B200 path-tracing engine (libwfb200.so).
+ *
+ * Plain pointers, sizes and opaque handles; no C++ types, no exceptions across the boundary.
+ * Every function returns a status (WFB_OK = 0) unless stated otherwise; the message of the last
+ * failure on the calling thread is returned by wfb_last_error().
+ *
+ * Each entry point names the reference interface it replaces (paths inside the reference
+ * project us-llm-engineer/graphics-book-tutorials, WVM = wavefront-vs-megakernel-path-tracing).
+ * Host array layouts are the reference's public structs (WVM/include/wf/scene.hpp:12-100):
+ *   sphere 32 B {float center[3], radius; int material, pad[3]}
+ *   vertex 12 B {float x, y, z}
+ *   triangle 16 B {int i0, i1, i2, material}
+ *   material 48 B {int type; float ior, pad0, pad1; float albedo[3], pad2; float emission[3], pad3}
+ *   BVH node 48 B {float lo[3]; int skip; float hi[3]; int prim_start, prim_count, pad[3]}
+ *   light 16 B {int prim; float area, pad[2]}
+ */
+#ifndef WFB200_H
+#define WFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WFB_ABI_VERSION 1
+
+/* Status codes. */
+#define WFB_OK 0
+#define WFB_ERR_INVALID_ARGUMENT 1 /* bad handle, size, index or parameter */
+#define WFB_ERR_CUDA 2             /* a CUDA runtime call failed (message has the CUDA string) */
+#define WFB_ERR_OUT_OF_MEMORY 3    /* device allocation failed or a memory budget is exceeded */
+#define WFB_ERR_NOT_FINALIZED 4    /* scene has no BVH nodes (reference: std::runtime_error) */
+#define WFB_ERR_UNSUPPORTED 5      /* valid input outside this engine's packed limits */
+#define WFB_ERR_TIMEOUT 6          /* a host-side wait ended before completion */
+#define WFB_ERR_DEVICE_WAIT 7      /* a bounded device-side wait gave up (kernel returned early) */
+#define WFB_ERR_INTERNAL 8
+
+#define WFB_MODE_MEGAKERNEL 0 /* wf::GpuMode::Megakernel */
+#define WFB_MODE_WAVEFRONT 1  /* wf::GpuMode::Wavefront */
+
+typedef struct wfb_scene* wfb_scene_t;
+typedef struct wfb_renderer* wfb_renderer_t;
+
+/* Library */
+int wfb_abi_version(void);
+const char* wfb_last_error(void);
+/* Writes the CUDA device name; replaces wf::GpuRenderer::device_name (WVM/src/gpu/gpu_renderer.cu:379-390). */
+int wfb_device_name(char* buf, int len);
+
+/* ---- scenes ---------------------------------------------------------------------------------
+ * Host description of a scene in the reference layouts. n_nodes == 0 means "not finalized". */
+typedef struct {
+    const void* spheres;     int n_spheres;
+    const float* vertices;   int n_vertices;
+    const int* triangles;    int n_triangles;
+    const void* materials;   int n_materials;
+    const void* nodes;       int n_nodes;
+    const int* prim_order;   int n_prim_order;
+    const void* lights;      int n_lights;
+    float env[3];
+    float cam_position[3];
+    float cam_look_at[3];
+    float cam_up[3];
+    float cam_vfov_deg;
+    int width, height;
+} wfb_scene_desc;
+
+typedef struct {
+    int n_spheres, n_vertices, n_triangles, n_materials, n_nodes, n_prim_order, n_lights;
+    int width, height;
+    float env[3];
+    float cam_position[3], cam_look_at[3], cam_up[3], cam_vfov_deg;
+} wfb_scene_info;
+
+/* Copies the description. finalize_bins == 0: the scene must already be finalized (its nodes,
+ * prim_order and lights are used as given, like wf::GpuRenderer's constructor,
+ * WVM/src/gpu/gpu_renderer.cu:100-104); finalize_bins > 0: validate, collect lights and build the
+ * BVH with that many SAH bins, like wf::finalize_scene (WVM/src/scene.cpp:58-104; 8 bins reproduces
+ * the reference tree). The scene is uploaded to the current device on first use. */
+int wfb_scene_create(const wfb_scene_desc* desc, int finalize_bins, wfb_scene_t* out);
+/* Procedural benchmark scene "cornell36", "icospheres" or "heightfield" (no reference
+ * counterpart: the reference's make_scene, WVM/src/scenes.cpp:29, has other scenes). */
+int wfb_scene_generate(const char* name, int width, int height, uint32_t seed, int sah_bins,
+                       wfb_scene_t* out);
+int wfb_scene_info_get(wfb_scene_t scene, wfb_scene_info* info);
+/* Copies the finalized host arrays into caller buffers sized from wfb_scene_info (any pointer
+ * may be NULL to skip that array). */
+int wfb_scene_export(wfb_scene_t scene, void* spheres, float* vertices, int* triangles,
+                     void* materials, void* nodes, int* prim_order, void* lights);
+/* Replaces wf::scene_hash (WVM/src/scene.cpp:107-160). */
+uint64_t wfb_scene_hash(wfb_scene_t scene);
+/* Replaces wf::validate_bvh (WVM/src/bvh_build.cpp:253-323): writes "" when valid. */
+int wfb_scene_validate_bvh(wfb_scene_t scene, char* msg, int len);
+/* Releases the caller's reference; device arrays live until the last renderer using them is gone. */
+int wfb_scene_destroy(wfb_scene_t scene);
+/* Device bytes of the resident (uploaded) scene; 0 before the first upload. */
+uint64_t wfb_scene_device_bytes(wfb_scene_t scene);
+
+/* ---- renderer: the wf::GpuRenderer class (WVM/include/wf/renderer.hpp:44-67) ----------------- */
+typedef struct {
+    int spp;
+    uint32_t seed;
+    int max_depth;
+    int count_rays;
+    int stage_timing;
+    int queue_capacity;
+} wfb_render_params; /* wf::RenderParams (WVM/include/wf/renderer.hpp:11-21) */
+
+typedef struct {
+    double render_ms;
+    double total_ms;
+    uint64_t extension_rays, shadow_rays;
+    int64_t queue_high_water[5];
+    int64_t queue_overflows;
+    int64_t invalid_hits;
+    uint64_t peak_vram_bytes;
+    double stage_ms[8]; /* extend, classify, lambert, metal, dielectric, shadow, compact, other */
+} wfb_render_stats; /* wf::RenderStats (WVM/include/wf/renderer.hpp:23-37) */
+
+/* GpuRenderer(const Scene&, GpuMode) (WVM/src/gpu/gpu_renderer.cu:100-238). */
+int wfb_renderer_create(wfb_scene_t scene, int mode, wfb_renderer_t* out);
+/* Camera and resolution of the scene by default; this overrides them (film is reallocated and
+ * zeroed). No reference counterpart (the reference binds the camera to the Scene). */
+int wfb_renderer_set_camera(wfb_renderer_t r, const float position[3], const float look_at[3],
+                            const float up[3], float vfov_deg, int width, int height);
+/* GpuRenderer::reset (WVM/src/gpu/gpu_renderer.cu:242-252). */
+int wfb_renderer_reset(wfb_renderer_t r);
+/* GpuRenderer::run_passes (WVM/src/gpu/gpu_renderer.cu:254-304): adds samples
+ * [first_sample, first_sample + count) to the film. stats may be NULL. */
+int wfb_renderer_run_passes(wfb_renderer_t r, int first_sample, int count,
+                            const wfb_render_params* p, wfb_render_stats* stats);
+/* GpuRenderer::download (WVM/src/gpu/gpu_renderer.cu:306-341): rgb = sum * (1/spp) in float,
+ * lum_var = max(0, E[l^2] - E[l]^2) in double. rgb: 3*w*h floats, lum_var: w*h (may be NULL). */
+int wfb_renderer_download(wfb_renderer_t r, int spp_done, float* rgb, float* lum_var);
+/* GpuRenderer::download_mean (WVM/src/gpu/gpu_renderer.cu:343-353). */
+int wfb_renderer_download_mean(wfb_renderer_t r, int spp_done, float* rgb);
+/* Raw film sums (rgb 3*w*h, lum w*h, lum2 w*h), the bit-exact comparison surface. */
+int wfb_renderer_download_sums(wfb_renderer_t r, float* rgb_sum, float* lum_sum, float* lum2_sum);
+/* GpuRenderer::render (WVM/src/gpu/gpu_renderer.cu:355-364): reset, run_passes(0, spp), download. */
+int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render_stats* stats,
+                        float* rgb, float* lum_var);
+/* GpuRenderer::device_bytes (WVM/src/gpu/gpu_renderer.cu:366-377). */
+uint64_t wfb_renderer_device_bytes(wfb_renderer_t r);
+int wfb_renderer_width(wfb_renderer_t r);
+int wfb_renderer_height(wfb_renderer_t r);
+/* ~GpuRenderer. */
+int wfb_renderer_destroy(wfb_renderer_t r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WFB200_H */

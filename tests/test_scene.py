@@ -1,0 +1,93 @@
+"""Scene model, BVH builder and hashes (CPU only)."""
+import numpy as np
+import pytest
+
+from conftest import load_engine
+
+
+def test_generated_scene_sizes(wfb):
+    c = wfb.Scene.generate("cornell36", 32, 18).info()
+    assert (c.n_triangles, c.n_spheres, c.n_lights) == (36, 0, 2)
+    i = wfb.Scene.generate("icospheres", 32, 18).info()
+    assert i.n_triangles == 2 + 2 + 512 * 320 and i.n_vertices == 8 + 512 * 162
+
+
+@pytest.mark.slow
+def test_heightfield_size(wfb):
+    h = wfb.Scene.generate("heightfield", 32, 18).info()
+    assert h.n_triangles == 2 * 1023 * 1023 + 2 and h.n_vertices == 1024 * 1024 + 4
+
+
+def test_generators_are_deterministic(wfb):
+    a = wfb.Scene.generate("icospheres", 32, 18, 1234)
+    b = wfb.Scene.generate("icospheres", 32, 18, 1234)
+    c = wfb.Scene.generate("icospheres", 32, 18, 4321)
+    assert a.hash() == b.hash() != c.hash()
+    # pinned values at the benchmark resolutions: any change to a generator shows up here
+    assert wfb.Scene.generate("cornell36", 320, 180, 1234).hash() == 0xda3d860077520452
+    assert wfb.Scene.generate("icospheres", 1280, 720, 1234).hash() == 0x1a1df472c06da555
+
+
+@pytest.mark.parametrize("name", ["cornell36", "icospheres"])
+@pytest.mark.parametrize("bins", [8, 16, 32])
+def test_bvh_is_valid(wfb, name, bins):
+    s = wfb.Scene.generate(name, 16, 9, 1234, bins)
+    assert s.validate_bvh() == ""
+    a = s.export()
+    # leaves <= 4, prim_order a permutation, skip links forward
+    leaves = a["nodes"][a["nodes"]["prim_count"] > 0]
+    assert leaves["prim_count"].max() <= 4
+    assert np.array_equal(np.sort(a["prim_order"]), np.arange(len(a["triangles"]) + len(a["spheres"])))
+
+
+@pytest.mark.parametrize("name", ["cornell36", "icospheres"])
+def test_8bin_builder_reproduces_reference_tree(ref, wfb, name):
+    """sah_bins == 8 is the reference-compatible policy: identical nodes and prim_order bytes."""
+    arrays = wfb.Scene.generate(name, 16, 9, 1234, 16).export()
+    bare = dict(arrays, nodes=None, prim_order=None, lights=None)
+    mine = wfb.Scene.from_arrays(bare, finalize_bins=8).export()
+    nodes, order = ref.ref_build_bvh(bare)
+    assert np.array_equal(mine["nodes"].view(np.uint8), nodes.view(np.uint8))
+    assert np.array_equal(mine["prim_order"], order)
+
+
+@pytest.mark.parametrize("name", ["cornell", "divergence", "trianglehv", "furnace"])
+def test_8bin_builder_on_reference_scenes(ref, wfb, name):
+    arrays = ref.ref_make_scene(name, 32, 18)
+    bare = dict(arrays, nodes=None, prim_order=None, lights=None)
+    mine = wfb.Scene.from_arrays(bare, finalize_bins=8).export()
+    assert np.array_equal(mine["nodes"].view(np.uint8), arrays["nodes"].view(np.uint8))
+    assert np.array_equal(mine["prim_order"], arrays["prim_order"])
+    assert np.array_equal(mine["lights"].view(np.uint8), arrays["lights"].view(np.uint8))
+
+
+@pytest.mark.parametrize("name,pin", [("cornell", 0x2ec1deb9ff15147d), ("divergence", 0x9f8c9de445c74762),
+                                      ("trianglehv", 0xa489bc1b27791a9d)])
+def test_scene_hash_matches_published_pins(ref, wfb, name, pin):
+    """scene_hash of the reference scenes at 1280x720 equals the values in the reference's bench results."""
+    arrays = ref.ref_make_scene(name, 1280, 720)
+    assert ref.ref_scene_hash(arrays) == pin
+    assert wfb.Scene.from_arrays(arrays).hash() == pin
+
+
+def test_unfinalized_scene_is_rejected(wfb):
+    arrays = wfb.Scene.generate("cornell36", 16, 9).export()
+    s = wfb.Scene.from_arrays(dict(arrays, nodes=None, prim_order=None, lights=None), finalize_bins=0)
+    with pytest.raises(wfb.WfbError) as e:
+        wfb.GpuRenderer(s, wfb.MEGAKERNEL)
+    assert e.value.status == wfb.ERR_NOT_FINALIZED
+
+
+def test_invalid_scene_messages(wfb):
+    arrays = wfb.Scene.generate("cornell36", 16, 9).export()
+    bad = dict(arrays, nodes=None, prim_order=None, lights=None)
+    t = bad["triangles"].copy()
+    t["material"][0] = 99
+    with pytest.raises(wfb.WfbError, match="triangle material index out of range"):
+        wfb.Scene.from_arrays(dict(bad, triangles=t), finalize_bins=8)
+    v = bad["vertices"].copy()
+    v[0, 0] = np.inf
+    with pytest.raises(wfb.WfbError, match="vertex is non-finite"):
+        wfb.Scene.from_arrays(dict(bad, vertices=v), finalize_bins=8)
+    with pytest.raises(wfb.WfbError, match="no primitives"):
+        wfb.Scene.from_arrays(dict(bad, triangles=bad["triangles"][:0]), finalize_bins=8)
