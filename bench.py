@@ -201,8 +201,17 @@ def main():
     ap.add_argument("--arm", default="megakernel", choices=["megakernel", "wavefront"])
     ap.add_argument("--ref-spp", type=int, default=2, help="samples per pixel of one reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--size", default=None, help="WxH override (profiling cases only; not a bench line)")
+    ap.add_argument("--spp", type=int, default=None, help="spp override (profiling cases only)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global WIDTH, HEIGHT, SPP, WORKLOAD
+    if args.size:
+        WIDTH, HEIGHT = (int(v) for v in args.size.lower().split("x"))
+    if args.spp:
+        SPP = args.spp
+    WORKLOAD = f"{SCENE}-512 {WIDTH}x{HEIGHT} {SPP}spp depth{DEPTH} seed{SEED}"
     if args.impl == "reference":
         run_reference(args)
         return
@@ -254,7 +263,7 @@ def main():
     # e2e through the public API: host arrays -> scene upload -> render -> film back in host memory
     e2e_times = []
     h2d = d2h = 0
-    for i in range(args.warmup + args.steps):
+    for i in range(0 if args.no_e2e else args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s2 = wfb.Scene.from_arrays(host_arrays)
@@ -267,12 +276,14 @@ def main():
         d2h = 5 * WIDTH * HEIGHT * 4  # film sums rgb + lum + lum2
         r2.close()
         s2.close()
-    e2e_s = sum(e2e_times) / len(e2e_times)
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = samples * world / e2e_s / 1e6
+    e2e_value = None
+    if e2e_times:
+        e2e_s = sum(e2e_times) / len(e2e_times)
+        if dist is not None:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e_value = round(samples * world / e2e_s / 1e6, 3)
 
     peaks, peak_kind = measured_peaks()
     bytes_per_sample = 224.0 * ext_ps + 96.0 * sh_ps + 40.0
@@ -293,7 +304,7 @@ def main():
             "ext_rays_per_sample": round(ext_ps, 4), "shadow_rays_per_sample": round(sh_ps, 4),
             "kernel": "megakernel_persistent" if args.arm == "megakernel" else "wavefront_persistent",
         },
-        "e2e": {"value": round(e2e_value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": args.steps,
         "mrays_per_s": round((ext_ps + sh_ps) * value, 2),

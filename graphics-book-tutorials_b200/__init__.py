@@ -184,6 +184,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_renderer_download_sums": (i32, [vp, vp, vp, vp]),
         "wfb_renderer_render": (i32, [vp, ctypes.POINTER(_CRenderParams), ctypes.POINTER(_CRenderStats), vp, vp]),
         "wfb_renderer_device_bytes": (u64, [vp]),
+        "wfb_renderer_configure": (i32, [vp, i32, i32, i32, i32, i32]),
         "wfb_renderer_width": (i32, [vp]),
         "wfb_renderer_height": (i32, [vp]),
         "wfb_renderer_destroy": (i32, [vp]),
@@ -363,6 +364,12 @@ class GpuRenderer:
 
     def device_bytes(self) -> int:
         return int(load_library().wfb_renderer_device_bytes(self._h))
+
+    def configure(self, block: int = 0, blocks_per_sm: int = 0, min_active: int = 0, split_chunks: int = 0,
+                  paths_in_flight: int = 0) -> None:
+        """Launch knobs (values <= 0 keep the current setting); see wfb_renderer_configure."""
+        _check(load_library().wfb_renderer_configure(self._h, block, blocks_per_sm, min_active, split_chunks,
+                                                      paths_in_flight))
 
     def close(self) -> None:
         if self._h is not None and self._h.value:

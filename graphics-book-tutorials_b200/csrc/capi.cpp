@@ -290,6 +290,16 @@ int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render
 }
 
 uint64_t wfb_renderer_device_bytes(wfb_renderer_t r) { return r ? r->r->device_bytes() : 0; }
+
+int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int min_active, int split_chunks,
+                           int paths_in_flight) {
+    return guarded([&] {
+        need(r != nullptr, "null renderer");
+        need(block <= 0 || block == 64 || block == 128 || block == 256, "block must be 64, 128 or 256");
+        need(min_active <= 32, "min_active must be in 1..32");
+        r->r->configure(block, blocks_per_sm, min_active, split_chunks, paths_in_flight);
+    });
+}
 int wfb_renderer_width(wfb_renderer_t r) { return r ? r->r->width() : 0; }
 int wfb_renderer_height(wfb_renderer_t r) { return r ? r->r->height() : 0; }
 

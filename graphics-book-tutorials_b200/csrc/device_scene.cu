@@ -81,6 +81,9 @@ std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
             leaf = (n.prim_start << kLeafCountBits) | n.prim_count;
         }
         if (n.skip < -1 || n.skip >= nn) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link out of bounds");
+        // Every traversal step moves forward (to N+1 or to a forward skip), so a traversal ends
+        // after at most n_nodes steps; a backward skip could loop forever and is rejected.
+        if (n.skip != -1 && n.skip <= i) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link does not point forward");
         nodes[2 * i] = f4(n.lo, i2f(n.skip));
         nodes[2 * i + 1] = f4(n.hi, i2f(leaf));
     }

@@ -50,13 +50,20 @@ struct PassParams {
 
 // ---- megakernel (megakernel.cu) ----
 struct MegakernelConfig {
-    int block = 128;     // threads per block
-    int blocks_per_sm = 0;  // 0: maximum resident
+    int block = 128;        // threads per CTA (64, 128 or 256)
+    int blocks_per_sm = 0;  // 0: as many as fit
+    int min_active = 20;    // traverse on while at least this many lanes of a warp traverse
+    int split_chunks = 0;   // work units per pixel; 0: chosen from pixels vs resident lanes
 };
-// Renders samples [first, first + count) of every pixel into `film` (adding to its sums).
+// Resident threads of the persistent megakernel for this configuration.
+int megakernel_resident_threads(const MegakernelConfig& cfg);
+// Work units per pixel (1 = direct film accumulation; > 1 needs a per-sample buffer).
+int megakernel_split_chunks(int pixels, int sample_count, const MegakernelConfig& cfg);
+// Adds samples [first, first + count) of every pixel to `film`. With chunks > 1, `lbuf` must hold
+// 3 * pixels * count floats (per-sample radiance, committed in sample order after the kernel).
 void launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters,
-                       unsigned int* work_counter, const PassParams& p,
-                       const MegakernelConfig& cfg, cudaStream_t stream);
+                       unsigned int* work_counter, float* lbuf, const PassParams& p,
+                       const MegakernelConfig& cfg, int chunks, cudaStream_t stream);
 
 // ---- GPU renderer (renderer.cu): one scene, one camera, one film ----
 class Renderer {
@@ -79,6 +86,9 @@ public:
     int pixels() const { return width_ * height_; }
     wf::GpuMode mode() const { return mode_; }
     void set_megakernel_config(const MegakernelConfig& c) { mk_cfg_ = c; }
+    const MegakernelConfig& megakernel_config() const { return mk_cfg_; }
+    // Values <= 0 keep the current setting.
+    void configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight);
 
 private:
     void alloc_film();
@@ -90,6 +100,8 @@ private:
     DevFilm film_{};
     DevCounters* counters_ = nullptr;
     unsigned int* work_ = nullptr;
+    float* lbuf_ = nullptr;  // split-mode per-sample radiance
+    size_t lbuf_floats_ = 0;
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     MegakernelConfig mk_cfg_{};

@@ -33,6 +33,7 @@ Renderer::~Renderer() {
     wf_.reset();
     if (counters_) cudaFree(counters_);
     if (work_) cudaFree(work_);
+    if (lbuf_) cudaFree(lbuf_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -81,7 +82,18 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
     cuda_check(cudaMemsetAsync(counters_, 0, sizeof(DevCounters), stream_), "zero counters");
     cuda_check(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
     if (mode_ == wf::GpuMode::Megakernel) {
-        launch_megakernel(view_, film_, counters_, work_, p, mk_cfg_, stream_);
+        const int chunks = megakernel_split_chunks(pixels(), p.sample_count, mk_cfg_);
+        if (chunks > 1) {
+            const size_t need = 3 * (size_t)pixels() * (size_t)p.sample_count;
+            if (need > lbuf_floats_) {
+                if (lbuf_) cudaFree(lbuf_);
+                lbuf_ = nullptr;
+                lbuf_floats_ = 0;
+                cuda_check(cudaMalloc(&lbuf_, need * sizeof(float)), "cudaMalloc sample buffer");
+                lbuf_floats_ = need;
+            }
+        }
+        launch_megakernel(view_, film_, counters_, work_, lbuf_, p, mk_cfg_, chunks, stream_);
     } else {
         wf_->engine.run(view_, film_, counters_, p, stats ? &stats->stages : nullptr, stream_);
     }
@@ -135,6 +147,14 @@ void Renderer::download(int spp_done, float* rgb, float* lum_var) {
 }
 
 void Renderer::download_mean(int spp_done, float* rgb) { download(spp_done, rgb, nullptr); }
+
+void Renderer::configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight) {
+    if (block > 0) mk_cfg_.block = block;
+    if (blocks_per_sm > 0) mk_cfg_.blocks_per_sm = blocks_per_sm;
+    if (min_active > 0) mk_cfg_.min_active = min_active;
+    if (split_chunks > 0) mk_cfg_.split_chunks = split_chunks;
+    (void)paths_in_flight;  // wavefront pool size (see WavefrontEngine)
+}
 
 uint64_t Renderer::device_bytes() const {
     uint64_t b = scene_->bytes + 5ull * pixels() * sizeof(float) + sizeof(DevCounters);

@@ -144,6 +144,12 @@ int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render
                         float* rgb, float* lum_var);
 /* GpuRenderer::device_bytes (WVM/src/gpu/gpu_renderer.cu:366-377). */
 uint64_t wfb_renderer_device_bytes(wfb_renderer_t r);
+/* Launch configuration knobs (no reference counterpart; set by the autotuner). Any value <= 0
+ * keeps the current setting. Megakernel: block 64/128/256 threads, CTAs per SM, the minimum
+ * number of traversing lanes per warp before shading runs (1..32), work units per pixel.
+ * Wavefront: block, paths in flight. */
+int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int min_active,
+                           int split_chunks, int paths_in_flight);
 int wfb_renderer_width(wfb_renderer_t r);
 int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */

@@ -132,3 +132,16 @@ def test_full_size_render_is_clean(wfb):
     assert st.invalid_hits == 0
     assert np.isfinite(out.rgb).all() and out.rgb.mean() > 0.0
     assert st.extension_rays >= 1280 * 720
+
+
+@pytest.mark.parametrize("block,min_active,split", [(64, 1, 1), (128, 32, 1), (256, 16, 3), (128, 20, 8)])
+def test_launch_configurations_give_identical_films(wfb, block, min_active, split):
+    """Block size, traversal threshold and direct/split accumulation never change a bit of the film."""
+    scene = wfb.Scene.generate("icospheres", 96, 54, 1234, 16)
+    p = wfb.RenderParams(spp=8, seed=21, max_depth=8)
+    base = wfb.GpuRenderer(scene, wfb.MEGAKERNEL).render(p)
+    r = wfb.GpuRenderer(scene, wfb.MEGAKERNEL)
+    r.configure(block=block, min_active=min_active, split_chunks=split)
+    out = r.render(p)
+    assert np.array_equal(bits(out.rgb), bits(base.rgb))
+    assert np.array_equal(bits(out.lum_var), bits(base.lum_var))
