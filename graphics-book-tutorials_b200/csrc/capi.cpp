@@ -5,6 +5,7 @@
 #include <mutex>
 #include <string>
 #include "engine.hpp"
+#include "noalloc.hpp"
 #include "scene_gen.hpp"
 #include "../../include/wfb200.h"
 
@@ -306,6 +307,23 @@ int wfb_renderer_height(wfb_renderer_t r) { return r ? r->r->height() : 0; }
 int wfb_renderer_destroy(wfb_renderer_t r) {
     delete r;
     return WFB_OK;
+}
+
+int wfb_render_passes_noalloc(wfb_scene_t s, int first_sample, int count, uint32_t seed, int max_depth,
+                              float* rgb_sum, float* lum_sum, float* lum2_sum, void* stream) {
+    return guarded([&] {
+        need(s != nullptr, "null scene");
+        std::shared_ptr<wfb::ResidentScene> rs;
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            rs = s->resident;  // never uploads here: uploading allocates
+        }
+        if (!rs)
+            throw wfb::Error(WFB_ERR_INVALID_ARGUMENT,
+                             "scene is not resident on the device; create a renderer on it first (that uploads it)");
+        wfb::render_passes_noalloc(*rs, first_sample, count, seed, max_depth, rgb_sum, lum_sum, lum2_sum,
+                                   static_cast<cudaStream_t>(stream));
+    });
 }
 
 }  // extern "C"

@@ -155,6 +155,27 @@ int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */
 int wfb_renderer_destroy(wfb_renderer_t r);
 
+/* ---- allocation-free rendering ---------------------------------------------------------------
+ * No counterpart in the reference. For callers that must not allocate device memory on their
+ * render path: a host that owns all device memory through its own pool, a real-time loop where
+ * an allocation (which can synchronise the device) would break the frame budget, or work issued
+ * while a stream is being captured into a CUDA graph (cudaMalloc is not allowed there).
+ *
+ * Adds samples [first_sample, first_sample + count) of `scene` -- its own camera and resolution
+ * w x h -- to caller-owned DEVICE film sums (rgb_sum 3*w*h floats, lum_sum w*h, lum2_sum w*h),
+ * exactly as wfb_renderer_run_passes adds them to a renderer's film (same bits). Enqueued on
+ * `stream` (a cudaStream_t; NULL = default stream); the call returns without waiting.
+ * Allocates nothing: its scratch is one static device array of about 12 MB that every GPU which
+ * loads the library holds until the process exits, and that all calls share. Calls that overlap
+ * on the GPU therefore race: serialise them (one stream, or wait between calls). The first call
+ * on a device looks up the array's address (cudaGetSymbolAddress); make that first call before
+ * any stream capture. The scene must already be resident on the current device (creating a
+ * renderer on it uploads it). Rejects w * h * count > WFB_NOALLOC_MAX_SAMPLES with
+ * WFB_ERR_INVALID_ARGUMENT; render larger requests in passes of fewer samples. */
+#define WFB_NOALLOC_MAX_SAMPLES 1048576
+int wfb_render_passes_noalloc(wfb_scene_t scene, int first_sample, int count, uint32_t seed, int max_depth,
+                              float* rgb_sum, float* lum_sum, float* lum2_sum, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
