@@ -188,6 +188,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_renderer_width": (i32, [vp]),
         "wfb_renderer_height": (i32, [vp]),
         "wfb_renderer_destroy": (i32, [vp]),
+        "wfb_scan_workspace_create": (i32, [i32, ctypes.POINTER(vp)]),
+        "wfb_scan_workspace_destroy": (i32, [vp]),
+        "wfb_scan_exclusive_u32": (i32, [vp, vp, i32, vp, vp, vp]),
+        "wfb_compact_u32": (i32, [vp, vp, vp, vp, vp, i32, vp, vp]),
+        "wfb_test_queue_push": (i32, [vp, i32, vp, u32, vp, vp, vp]),
+        "wfb_scan_workspace_check": (i32, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -404,3 +410,43 @@ def compare_results(a: RenderResult, b: RenderResult) -> dict:
     mean_rel = abs(mean_a - mean_b) / mean_a if mean_a > 1e-12 else abs(mean_a - mean_b)
     return {"max_abs_rel": float(rel.max()) if n else 0.0, "mean_rel": mean_rel,
             "frac_within_3se": float(within.mean()) if n else 0.0, "nonfinite": nonfinite}
+
+
+class ScanWorkspace:
+    """Queue primitives on device pointers (WVM/src/gpu/queues.cuh:30-55): single-pass
+    decoupled-look-back scan and stable compaction. Pointers are integers (e.g. tensor.data_ptr());
+    calls are stream-ordered and return the C status (0 = OK, 1 = n > capacity)."""
+
+    def __init__(self, capacity: int):
+        h = ctypes.c_void_p()
+        _check(load_library().wfb_scan_workspace_create(int(capacity), ctypes.byref(h)))
+        self._h = h
+        self.capacity = int(capacity)
+
+    def scan_exclusive_u32(self, d_in: int, d_out: int, n: int, d_total: int = 0, stream: int = 0) -> int:
+        return load_library().wfb_scan_exclusive_u32(d_in, d_out, n, d_total or None, self._h, stream or None)
+
+    def compact_u32(self, d_values: int, d_flags: int, d_out: int, d_count: int, n: int, stream: int = 0) -> int:
+        return load_library().wfb_compact_u32(d_values, d_flags, d_out, d_count or None, None, n, self._h,
+                                              stream or None)
+
+    def check(self, stream: int = 0) -> None:
+        _check(load_library().wfb_scan_workspace_check(self._h, stream or None))
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            load_library().wfb_scan_workspace_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def test_queue_push(d_flags: int, n: int, d_items: int, capacity: int, d_counter: int, d_overflow: int,
+                    stream: int = 0) -> int:
+    """test_queue_push (WVM/src/gpu/queues.cuh:53-54) on device pointers; returns the C status."""
+    return load_library().wfb_test_queue_push(d_flags, n, d_items or None, capacity & 0xFFFFFFFF, d_counter,
+                                              d_overflow, stream or None)

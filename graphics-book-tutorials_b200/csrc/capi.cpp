@@ -6,6 +6,7 @@
 #include <string>
 #include "engine.hpp"
 #include "noalloc.hpp"
+#include "queues.hpp"
 #include "scene_gen.hpp"
 #include "../../include/wfb200.h"
 
@@ -22,6 +23,10 @@ struct wfb_scene {
 
 struct wfb_renderer {
     std::unique_ptr<wfb::Renderer> r;
+};
+
+struct wfb_scan_workspace {
+    std::unique_ptr<wfb::ScanWorkspace> ws;
 };
 
 namespace {
@@ -307,6 +312,55 @@ int wfb_renderer_height(wfb_renderer_t r) { return r ? r->r->height() : 0; }
 int wfb_renderer_destroy(wfb_renderer_t r) {
     delete r;
     return WFB_OK;
+}
+
+int wfb_scan_workspace_create(int capacity, wfb_scan_workspace_t* out) {
+    return guarded([&] {
+        need(out != nullptr, "null argument");
+        auto w = std::make_unique<wfb_scan_workspace>();
+        w->ws = wfb::scan_workspace_create(capacity);
+        *out = w.release();
+    });
+}
+
+int wfb_scan_workspace_destroy(wfb_scan_workspace_t ws) {
+    delete ws;
+    return WFB_OK;
+}
+
+int wfb_scan_exclusive_u32(const uint32_t* d_in, uint32_t* d_out, int n, uint32_t* d_total, wfb_scan_workspace_t ws,
+                           void* stream) {
+    return guarded([&] {
+        need(ws != nullptr, "null workspace");
+        need(n == 0 || (d_in && d_out), "null buffer");
+        wfb::scan_exclusive_u32(d_in, d_out, n, d_total, *ws->ws, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int wfb_compact_u32(const uint32_t* d_values, const uint32_t* d_flags, uint32_t* d_out, uint32_t* d_count,
+                    uint32_t* d_scratch, int n, wfb_scan_workspace_t ws, void* stream) {
+    (void)d_scratch;
+    return guarded([&] {
+        need(ws != nullptr, "null workspace");
+        need(n == 0 || (d_values && d_flags && d_out), "null buffer");
+        wfb::compact_u32(d_values, d_flags, d_out, d_count, n, *ws->ws, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int wfb_test_queue_push(const uint32_t* d_flags, int n, uint32_t* d_items, uint32_t capacity, uint32_t* d_counter,
+                        uint32_t* d_overflow, void* stream) {
+    return guarded([&] {
+        need(n == 0 || (d_flags && d_counter && d_overflow && (capacity == 0 || d_items)), "null buffer");
+        wfb::test_queue_push(d_flags, n, d_items, capacity, d_counter, d_overflow, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int wfb_scan_workspace_check(wfb_scan_workspace_t ws, void* stream) {
+    return guarded([&] {
+        need(ws != nullptr, "null workspace");
+        if (wfb::scan_workspace_failed(*ws->ws, static_cast<cudaStream_t>(stream)))
+            throw wfb::Error(WFB_ERR_DEVICE_WAIT, "a scan look-back wait gave up");
+    });
 }
 
 int wfb_render_passes_noalloc(wfb_scene_t s, int first_sample, int count, uint32_t seed, int max_depth,

@@ -65,6 +65,16 @@ void launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* coun
                        unsigned int* work_counter, float* lbuf, const PassParams& p,
                        const MegakernelConfig& cfg, int chunks, cudaStream_t stream);
 
+// Adds per-(pixel, sample) radiance slots (3 floats, pixel-major, `count` samples per pixel) to the
+// film sums in ascending sample order (megakernel.cu).
+void launch_film_commit(const DevFilm& film, const float* lbuf, int count, cudaStream_t stream);
+
+// ---- wavefront (wavefront.cu) ----
+struct WavefrontConfig {
+    int paths_in_flight = 0;  // path-pool slots; 0: 1M (capped at 64 x pixels)
+    int min_active = 20;      // traverse on while at least this many lanes of a warp traverse
+};
+
 // ---- GPU renderer (renderer.cu): one scene, one camera, one film ----
 class Renderer {
 public:
@@ -105,6 +115,7 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     MegakernelConfig mk_cfg_{};
+    WavefrontConfig wf_cfg_{};
     struct Wavefront;
     std::unique_ptr<Wavefront> wf_;
 };

@@ -319,6 +319,12 @@ void launch_block(const MkArgs& args, int blocks_per_sm, cudaStream_t stream) {
 
 }  // namespace
 
+void launch_film_commit(const DevFilm& film, const float* lbuf, int count, cudaStream_t stream) {
+    if (film.pixels <= 0 || count <= 0) return;
+    film_commit<<<(film.pixels + 255) / 256, 256, 0, stream>>>(film, lbuf, film.pixels, count);
+    cuda_check(cudaGetLastError(), "film commit launch");
+}
+
 int megakernel_resident_threads(const MegakernelConfig& cfg) {
     switch (cfg.block) {
         case 64: return 64 * resident_lanes<64>(cfg.blocks_per_sm);

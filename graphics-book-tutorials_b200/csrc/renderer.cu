@@ -10,8 +10,9 @@
 namespace wfb {
 
 struct Renderer::Wavefront {
+    WavefrontConfig cfg;
     WavefrontEngine engine;
-    explicit Wavefront(int pixels) : engine(pixels) {}
+    Wavefront(int pixels, const WavefrontConfig& c) : cfg(c), engine(pixels, c) {}
 };
 
 Renderer::Renderer(std::shared_ptr<ResidentScene> scene, wf::GpuMode mode)
@@ -48,7 +49,7 @@ void Renderer::alloc_film() {
     film_.lum2 = base + 4 * p;
     film_.pixels = (int)p;
     cuda_check(cudaMemset(base, 0, 5 * p * sizeof(float)), "cudaMemset film");
-    if (mode_ == wf::GpuMode::Wavefront) wf_ = std::make_unique<Wavefront>((int)p);
+    if (mode_ == wf::GpuMode::Wavefront) wf_ = std::make_unique<Wavefront>((int)p, wf_cfg_);
 }
 
 void Renderer::free_film() {
@@ -153,7 +154,13 @@ void Renderer::configure(int block, int blocks_per_sm, int min_active, int split
     if (blocks_per_sm > 0) mk_cfg_.blocks_per_sm = blocks_per_sm;
     if (min_active > 0) mk_cfg_.min_active = min_active;
     if (split_chunks > 0) mk_cfg_.split_chunks = split_chunks;
-    (void)paths_in_flight;  // wavefront pool size (see WavefrontEngine)
+    if (mode_ == wf::GpuMode::Wavefront && (paths_in_flight > 0 || min_active > 0)) {
+        if (paths_in_flight > 0) wf_cfg_.paths_in_flight = paths_in_flight;
+        if (min_active > 0) wf_cfg_.min_active = min_active;
+        cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+        wf_.reset();
+        wf_ = std::make_unique<Wavefront>(pixels(), wf_cfg_);
+    }
 }
 
 uint64_t Renderer::device_bytes() const {

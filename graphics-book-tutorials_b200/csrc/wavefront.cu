@@ -1,20 +1,713 @@
-// Persistent-threads wavefront engine (implementation in progress).
+// Persistent-threads wavefront: the whole render is ONE cooperative launch that iterates bounces on
+// the device. Replaces the reference's wavefront (WVM/src/gpu/wavefront.cu:30-601), which launches
+// 12+ kernels per bounce and synchronises the host 3 times per bounce.
+//
+// Path pool: `capacity` slots, structure of arrays (one array per field, coalesced by slot id),
+// sized by paths_in_flight so that the pool can stay L2-resident. A slot owns a work unit (a pixel
+// and a run of its samples, as in the megakernel) and, when its path ends, regenerates the next
+// sample of the same pixel or takes a new unit: paths in flight stay constant until the work runs
+// out. Film sums are kept per slot in sample order (direct mode) or per (pixel, sample) in a
+// buffer committed in order afterwards (split mode), so the film is bit-identical to every arm.
+//
+// One bounce = five phases separated by grid barriers (bounded spins, error flag on timeout):
+//   R  regenerate + compact: ended slots commit their sample and start the next one (or fetch a
+//      unit, or go idle); a decoupled-look-back scan over the active list writes the next active
+//      list, stable, and its length.
+//   E  extend: closest-hit traversal of every active path, lanes fetching rays dynamically from
+//      the active list (one atomic per warp per refill) and stepping a resumable stackless
+//      traversal, so a warp never waits for its longest ray.
+//   C  classify: validity check, emission/MIS/termination; slots pushed to the Lambertian, metal or
+//      dielectric queue with warp-aggregated pushes (drop-and-count past the test capacity).
+//   S  shade: the three material queues (shade_lambert pushes shadow records).
+//   H  shadow: any-hit traversal of the shadow queue with dynamic fetch; unoccluded contributions
+//      are added to the path radiance (a slot has at most one shadow record per bounce).
+// Stage times come from %globaltimer at the barriers (no host synchronisation).
+#include <algorithm>
+#include <cstring>
+#include "engine.hpp"
+#include "queues.cuh"
 #include "wavefront.hpp"
 #include "../../include/wfb200.h"
 
 namespace wfb {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWfBlock = 256;
+constexpr int kStages = 8;  // extend, classify, lambert, metal, dielectric, shadow, compact, other
+
+struct Control {
+    unsigned bar_count;
+    unsigned bar_gen;
+    unsigned n_active;
+    unsigned n_next;
+    unsigned qcount[4];  // lambert, metal, dielectric, shadow
+    unsigned fetch[2];   // extend, shadow dynamic-fetch cursors
+    unsigned unit_next;
+    unsigned ticket;
+    unsigned err;
+    unsigned overflow;
+    unsigned invalid;
+    unsigned high_water[5];
+    unsigned long long ext_rays;
+    unsigned long long shadow_rays;
+    unsigned long long stage_ns[kStages];
+};
+
+struct Pool {
+    float4* ray_o;   // origin, tmin
+    float4* ray_d;   // direction, tmax
+    float4* thr;     // throughput, prev_pdf
+    float4* rad;     // L, depth | specular << 30
+    uint2* key;
+    int4* unit;      // pixel (-1: none), sample, end sample, 0
+    float4* acc;     // film sums of the unit (direct mode): rgb, lum
+    float* acc2;     // lum2
+    float4* hit;     // t, prim, u, v
+    float4* surf_p;  // p, material | inside << 31
+    float4* surf_n;  // n
+    uint32_t* alive;
+    uint32_t* list[2];
+    uint32_t* queue[4];  // lambert, metal, dielectric, shadow slots
+    float4* sh_dir;      // shadow records: direction, tmax
+    float4* sh_c;        // contribution, owner slot
+    unsigned long long* status;
+    Control* ctl;
+};
+
+struct WfArgs {
+    DevScene s;
+    DevFilm film;
+    Pool pool;
+    float* lbuf;
+    int capacity;
+    int pixels;
+    int first_sample;
+    int sample_count;
+    int chunk;
+    int chunks;
+    uint32_t seed;
+    int max_depth;
+    uint32_t qcap;  // queue capacity (test hook); capacity otherwise
+    int min_active;
+    int split_shading;  // stage timing: a barrier between material queues
+};
+
+__device__ __forceinline__ wf::PathState load_path(const Pool& P, int slot) {
+    const float4 o = P.ray_o[slot], d = P.ray_d[slot], t = P.thr[slot], l = P.rad[slot];
+    const uint2 k = P.key[slot];
+    wf::PathState ps;
+    ps.ray.o = wf::Vec3{o.x, o.y, o.z};
+    ps.ray.tmin = o.w;
+    ps.ray.d = wf::Vec3{d.x, d.y, d.z};
+    ps.ray.tmax = d.w;
+    ps.throughput = wf::Vec3{t.x, t.y, t.z};
+    ps.prev_pdf = t.w;
+    ps.L = wf::Vec3{l.x, l.y, l.z};
+    const int bits = __float_as_int(l.w);
+    ps.depth = bits & 0x3fffffff;
+    ps.specular = (bits >> 30) & 1;
+    ps.key.k0 = k.x;
+    ps.key.k1 = k.y;
+    return ps;
+}
+
+__device__ __forceinline__ void store_path(const Pool& P, int slot, const wf::PathState& ps) {
+    P.ray_o[slot] = make_float4(ps.ray.o.x, ps.ray.o.y, ps.ray.o.z, ps.ray.tmin);
+    P.ray_d[slot] = make_float4(ps.ray.d.x, ps.ray.d.y, ps.ray.d.z, ps.ray.tmax);
+    P.thr[slot] = make_float4(ps.throughput.x, ps.throughput.y, ps.throughput.z, ps.prev_pdf);
+    P.rad[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, __int_as_float(ps.depth | (ps.specular << 30)));
+    P.key[slot] = make_uint2(ps.key.k0, ps.key.k1);
+}
+
+__device__ __forceinline__ void store_radiance(const Pool& P, int slot, const wf::PathState& ps) {
+    P.rad[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, __int_as_float(ps.depth | (ps.specular << 30)));
+}
+
+// Grid-wide barrier over co-resident CTAs (cooperative launch). Bounded: a wait longer than
+// kSpinLimitNs, or an error raised elsewhere, makes every CTA leave with `false`.
+__device__ bool grid_sync(Control* c, unsigned nblocks, int stage, unsigned long long* t_last) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* gen = &c->bar_gen;
+        const unsigned g = *gen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(&c->bar_count, 1u) == nblocks - 1) {
+            c->bar_count = 0;
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            while (*gen == g) {
+                if (*(volatile unsigned*)&c->err != 0u || global_ns() - t0 > kSpinLimitNs) {
+                    atomicExch(&c->err, 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if (*(volatile unsigned*)&c->err != 0u) ok = 0;
+        if (blockIdx.x == 0 && stage >= 0) {
+            const unsigned long long now = global_ns();
+            c->stage_ns[stage] += now - *t_last;
+            *t_last = now;
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Resumable closest-hit / any-hit traversal over a list of rays fetched dynamically.
+// Extend: items[i] are slot ids. Shadow: the rays are shadow records 0..n-1 (items unused).
+template <bool SHADOW>
+__device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned n, unsigned* cursor,
+                               unsigned long long* n_rays) {
+    const DevScene& s = a.s;
+    const Pool& P = a.pool;
+    const int lane = threadIdx.x & 31;
+    int item = -1;  // list position, -1: none
+    uint32_t id = 0;  // slot (extend) or shadow record (shadow) of the current ray
+    int node = -1;
+    wf::Vec3 o{0, 0, 0}, rd{0, 0, 1}, inv_d{0, 0, 1};
+    float tmin = 0.f;
+    wf::HitRecord h;
+    h.t = 0.f;
+    h.prim = -1;
+    h.u = h.v = 0.f;
+    bool exhausted = false;
+    for (;;) {
+        // refill lanes without a ray
+        const bool need = item < 0 && !exhausted;
+        const unsigned nm = __ballot_sync(kFull, need);
+        if (nm) {
+            const int leader = __ffs(nm) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(cursor, (unsigned)__popc(nm));
+            base = __shfl_sync(kFull, base, leader);
+            if (need) {
+                const unsigned i = base + __popc(nm & ((1u << lane) - 1u));
+                if (i < n) {
+                    item = (int)i;
+                    id = SHADOW ? i : items[i];  // shadow records are numbered by queue position
+                    if (SHADOW) {
+                        const float4 d = P.sh_dir[id];
+                        const int slot = __float_as_int(P.sh_c[id].w);
+                        const float4 oo = P.ray_o[slot];
+                        o = wf::Vec3{oo.x, oo.y, oo.z};
+                        rd = wf::Vec3{d.x, d.y, d.z};
+                        tmin = wf::kRayEps;
+                        h.t = d.w;
+                    } else {
+                        const float4 oo = P.ray_o[id], d = P.ray_d[id];
+                        o = wf::Vec3{oo.x, oo.y, oo.z};
+                        tmin = oo.w;
+                        rd = wf::Vec3{d.x, d.y, d.z};
+                        h.t = d.w;
+                    }
+                    h.prim = -1;
+                    h.u = 0.0f;
+                    h.v = 0.0f;
+                    inv_d = wf::Vec3{1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
+                    node = s.n_nodes > 0 ? 0 : -1;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (__ballot_sync(kFull, item >= 0) == 0) return;
+        // step every traversing lane while enough lanes traverse (or nothing is left to fetch)
+        for (;;) {
+            const bool trav = node >= 0;
+            const unsigned tm = __ballot_sync(kFull, trav);
+            if (tm == 0) break;
+            if (__popc(tm) < a.min_active && __ballot_sync(kFull, !trav && !exhausted) != 0) break;
+            if (trav) {
+                const float4 na = __ldg(&s.nodes[2 * node]);
+                const float4 nb = __ldg(&s.nodes[2 * node + 1]);
+                const int skip = __float_as_int(na.w);
+                wf::Ray r;
+                r.o = o;
+                r.d = rd;
+                r.tmin = tmin;
+                r.tmax = h.t;
+                if (!wf::hit_box(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, r.o, inv_d, r.tmin, r.tmax)) {
+                    node = skip;
+                } else {
+                    const int leaf = __float_as_int(nb.w);
+                    if (leaf < 0) {
+                        node = node + 1;
+                    } else {
+                        node = skip;
+                        const int count = leaf & kLeafCountMask;
+                        const float4* rec = s.prims + 3 * (leaf >> kLeafCountBits);
+                        for (int i = 0; i < count; ++i, rec += 3) {
+                            const float4 q0 = __ldg(rec);
+                            const float4 q1 = __ldg(rec + 1);
+                            const int p = __float_as_int(q0.w);
+                            float t, u = 0.0f, v = 0.0f;
+                            bool hit;
+                            if (p < s.n_spheres) {
+                                hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
+                            } else {
+                                const float4 q2 = __ldg(rec + 2);
+                                hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
+                                                            wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
+                            }
+                            if (hit) {
+                                r.tmax = t;
+                                h.t = t;
+                                h.prim = p;
+                                h.u = u;
+                                h.v = v;
+                                if (SHADOW) {
+                                    node = -1;
+                                    break;
+                                }
+                            }
+                        }
+                    }
+                }
+                if (node >= s.n_nodes) node = -1;
+            }
+        }
+        // retire finished rays
+        if (item >= 0 && node < 0) {
+            ++*n_rays;
+            if (SHADOW) {
+                if (h.prim < 0) {  // unoccluded: L += contrib
+                    const float4 c = P.sh_c[id];
+                    const int slot = __float_as_int(c.w);
+                    float4 l = P.rad[slot];
+                    l.x += c.x;
+                    l.y += c.y;
+                    l.z += c.z;
+                    P.rad[slot] = l;
+                }
+            } else {
+                P.hit[id] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
+            }
+            item = -1;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a) {
+    const DevScene& s = a.s;
+    const Pool& P = a.pool;
+    Control* c = P.ctl;
+    const int lane = threadIdx.x & 31;
+    const unsigned nblocks = gridDim.x;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int gthreads = gridDim.x * blockDim.x;
+    const bool split = a.chunks > 1;
+    const unsigned total_units = (unsigned)a.pixels * (unsigned)a.chunks;
+    __shared__ uint32_t smem[33];
+    __shared__ int s_tile;
+    __shared__ uint32_t s_prefix;
+    unsigned long long t_last = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) t_last = global_ns();
+    unsigned long long n_ext = 0, n_sh = 0;
+    unsigned n_invalid = 0;
+
+    for (unsigned iter = 1;; ++iter) {
+        const int cur = (iter - 1) & 1;
+        const uint32_t* active = P.list[cur];
+        uint32_t* next = P.list[cur ^ 1];
+        const unsigned n_act = *(volatile unsigned*)&c->n_active;
+
+        // ---------------- R: regenerate ended paths, compact the active list ----------------
+        if (gtid == 0) {
+            c->qcount[0] = c->qcount[1] = c->qcount[2] = c->qcount[3] = 0;
+            c->fetch[0] = c->fetch[1] = 0;
+        }
+        const unsigned ntiles = (n_act + kWfBlock - 1) / kWfBlock;
+        for (;;) {
+            if (threadIdx.x == 0) s_tile = (int)atomicAdd(&c->ticket, 1u);
+            __syncthreads();
+            const int tile = s_tile;
+            if (tile >= (int)ntiles) break;
+            const unsigned i = (unsigned)tile * kWfBlock + threadIdx.x;
+            const bool valid = i < n_act;
+            const int slot = valid ? (int)active[i] : 0;
+            bool has_path = false, need_unit = false;
+            int4 u = make_int4(-1, 0, 0, 0);
+            if (valid) {
+                has_path = P.alive[slot] != 0u;
+                if (!has_path) {
+                    u = P.unit[slot];
+                    if (u.x >= 0) {
+                        // commit the finished sample (film_add order, WVM/src/gpu/engine.cuh:25-32)
+                        const float4 l = P.rad[slot];
+                        if (split) {
+                            float* dst = a.lbuf + 3 * ((size_t)u.x * a.sample_count + (u.y - a.first_sample));
+                            dst[0] = l.x;
+                            dst[1] = l.y;
+                            dst[2] = l.z;
+                        } else {
+                            float4 ac = P.acc[slot];
+                            float a2 = P.acc2[slot];
+                            ac.x += l.x;
+                            ac.y += l.y;
+                            ac.z += l.z;
+                            const float lu = wf::luminance(wf::Vec3{l.x, l.y, l.z});
+                            ac.w += lu;
+                            a2 += lu * lu;
+                            P.acc[slot] = ac;
+                            P.acc2[slot] = a2;
+                        }
+                        u.y += 1;
+                        if (u.y < u.z) {
+                            const int px = u.x % s.width, py = u.x / s.width;
+                            store_path(P, slot, wf::init_path(s, px, py, (uint32_t)u.y, a.seed));
+                            P.unit[slot] = u;
+                            P.alive[slot] = 1u;
+                            has_path = true;
+                        } else {
+                            if (!split) {
+                                const float4 ac = P.acc[slot];
+                                a.film.rgb[3 * u.x] = ac.x;
+                                a.film.rgb[3 * u.x + 1] = ac.y;
+                                a.film.rgb[3 * u.x + 2] = ac.z;
+                                a.film.lum[u.x] = ac.w;
+                                a.film.lum2[u.x] = P.acc2[slot];
+                            }
+                            u.x = -1;
+                            P.unit[slot] = u;
+                            need_unit = true;
+                        }
+                    } else {
+                        need_unit = true;
+                    }
+                }
+            }
+            // fetch new units for slots that need one (one atomic per warp)
+            const unsigned nm = __ballot_sync(kFull, need_unit);
+            if (nm) {
+                const int leader = __ffs(nm) - 1;
+                unsigned base = 0;
+                if (lane == leader) base = atomicAdd(&c->unit_next, (unsigned)__popc(nm));
+                base = __shfl_sync(kFull, base, leader);
+                if (need_unit) {
+                    const unsigned uid = base + __popc(nm & ((1u << lane) - 1u));
+                    if (uid < total_units) {
+                        const int pixel = (int)(uid % (unsigned)a.pixels);
+                        const int ch = (int)(uid / (unsigned)a.pixels);
+                        const int first = a.first_sample + ch * a.chunk;
+                        const int end = min(first + a.chunk, a.first_sample + a.sample_count);
+                        P.unit[slot] = make_int4(pixel, first, end, 0);
+                        if (!split) {
+                            P.acc[slot] = make_float4(a.film.rgb[3 * pixel], a.film.rgb[3 * pixel + 1],
+                                                      a.film.rgb[3 * pixel + 2], a.film.lum[pixel]);
+                            P.acc2[slot] = a.film.lum2[pixel];
+                        }
+                        store_path(P, slot, wf::init_path(s, pixel % s.width, pixel / s.width, (uint32_t)first, a.seed));
+                        P.alive[slot] = 1u;
+                        has_path = true;
+                    }
+                }
+            }
+            // stable compaction of the slots that still have a path
+            const uint32_t flag = (valid && has_path) ? 1u : 0u;
+            uint32_t agg;
+            const uint32_t excl = block_exclusive_sum(flag, smem, &agg);
+            if (threadIdx.x == 0) publish_status(P.status, tile, iter, tile == 0 ? kStatusPrefix : kStatusAggregate, agg);
+            if (tile > 0 && threadIdx.x < 32) {
+                const uint32_t pre = tile_lookback(P.status, tile, iter, &c->err);
+                if (threadIdx.x == 0) {
+                    publish_status(P.status, tile, iter, kStatusPrefix, pre + agg);
+                    s_prefix = pre;
+                }
+            } else if (tile == 0 && threadIdx.x == 0) {
+                s_prefix = 0;
+            }
+            __syncthreads();
+            if (flag) next[s_prefix + excl] = (uint32_t)slot;
+            if (tile == (int)ntiles - 1 && threadIdx.x == kWfBlock - 1) c->n_next = s_prefix + excl + flag;
+            __syncthreads();
+        }
+        if (ntiles == 0 && gtid == 0) c->n_next = 0;
+        if (!grid_sync(c, nblocks, 6, &t_last)) break;
+        const unsigned n = *(volatile unsigned*)&c->n_next;
+        if (gtid == 0) {
+            c->n_active = n;
+            c->ticket = 0;
+            if (n > c->high_water[4]) c->high_water[4] = n;
+        }
+        if (n == 0) break;
+
+        // ---------------- E: extension rays ----------------
+        traverse_phase<false>(a, next, n, &c->fetch[0], &n_ext);
+        if (!grid_sync(c, nblocks, 0, &t_last)) break;
+
+        // ---------------- C: classify, push material queues ----------------
+        for (unsigned base = (unsigned)blockIdx.x * kWfBlock; base < n; base += (unsigned)gthreads) {
+            const unsigned i = base + threadIdx.x;
+            const bool valid = i < n;
+            const int slot = valid ? (int)next[i] : 0;
+            int mat = -1;
+            if (valid) {
+                const float4 hv = P.hit[slot];
+                wf::HitRecord h;
+                h.t = hv.x;
+                h.prim = __float_as_int(hv.y);
+                h.u = hv.z;
+                h.v = hv.w;
+                if (!hit_is_valid(s, h)) {
+                    ++n_invalid;
+                    h.prim = -1;  // treated as a miss
+                }
+                wf::PathState ps = load_path(P, slot);
+                wf::Surface f;
+                mat = wf::classify(s, ps, h, a.max_depth, &f);
+                store_radiance(P, slot, ps);
+                if (mat >= 0) {
+                    P.surf_p[slot] = make_float4(f.p.x, f.p.y, f.p.z,
+                                                 __uint_as_float((unsigned)f.material | ((unsigned)f.inside << 31)));
+                    P.surf_n[slot] = make_float4(f.n.x, f.n.y, f.n.z, 0.0f);
+                } else {
+                    P.alive[slot] = 0u;
+                }
+            }
+            for (int q = 0; q < 3; ++q) {
+                const bool mine = valid && mat == q;
+                const uint32_t at = queue_push(P.queue[q], &c->qcount[q], a.qcap, (uint32_t)slot, mine, &c->overflow);
+                if (mine && at == 0xFFFFFFFFu) P.alive[slot] = 0u;  // dropped on overflow: the path ends
+            }
+        }
+        if (!grid_sync(c, nblocks, 1, &t_last)) break;
+
+        // ---------------- S: shade the three material queues ----------------
+        unsigned qn[3];
+        for (int q = 0; q < 3; ++q) qn[q] = min(*(volatile unsigned*)&c->qcount[q], a.qcap);
+        if (gtid == 0)
+            for (int q = 0; q < 3; ++q)
+                if (qn[q] > c->high_water[q]) c->high_water[q] = qn[q];
+        bool ok = true;
+        for (int q = 0; q < 3 && ok; ++q) {
+            for (unsigned base = (unsigned)blockIdx.x * kWfBlock; base < qn[q]; base += (unsigned)gthreads) {
+                const unsigned i = base + threadIdx.x;
+                const bool valid = i < qn[q];
+                bool push = false;
+                int slot = 0;
+                wf::Ray sh;
+                wf::Vec3 contrib{0.f, 0.f, 0.f};
+                if (valid) {
+                    slot = (int)P.queue[q][i];
+                    wf::PathState ps = load_path(P, slot);
+                    const float4 sp = P.surf_p[slot], sn = P.surf_n[slot];
+                    wf::Surface f;
+                    f.p = wf::Vec3{sp.x, sp.y, sp.z};
+                    const unsigned mi = __float_as_uint(sp.w);
+                    f.material = (int)(mi & 0x7fffffffu);
+                    f.inside = (int)(mi >> 31);
+                    f.n = wf::Vec3{sn.x, sn.y, sn.z};
+                    f.n_out = f.n;  // not used by the shading steps
+                    bool alive;
+                    if (q == wf::kLambert) {
+                        int has = 0;
+                        alive = wf::shade_lambert(s, ps, f, &sh, &contrib, &has);
+                        push = has != 0;
+                    } else if (q == wf::kMetal) {
+                        alive = wf::shade_metal(s, ps, f);
+                    } else {
+                        alive = wf::shade_dielectric(s, ps, f);
+                    }
+                    store_path(P, slot, ps);
+                    P.alive[slot] = alive ? 1u : 0u;
+                }
+                if (q == wf::kLambert) {
+                    const uint32_t at = queue_push(P.queue[3], &c->qcount[3], a.qcap, (uint32_t)slot, push, &c->overflow);
+                    if (push && at != 0xFFFFFFFFu) {
+                        P.sh_dir[at] = make_float4(sh.d.x, sh.d.y, sh.d.z, sh.tmax);
+                        P.sh_c[at] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(slot));
+                    }
+                }
+            }
+            if (a.split_shading && !grid_sync(c, nblocks, 2 + q, &t_last)) ok = false;
+        }
+        if (!ok) break;
+        if (!a.split_shading && !grid_sync(c, nblocks, 2, &t_last)) break;
+
+        // ---------------- H: shadow rays ----------------
+        const unsigned nsh = min(*(volatile unsigned*)&c->qcount[3], a.qcap);
+        if (gtid == 0 && nsh > c->high_water[3]) c->high_water[3] = nsh;
+        traverse_phase<true>(a, nullptr, nsh, &c->fetch[1], &n_sh);
+        if (!grid_sync(c, nblocks, 5, &t_last)) break;
+    }
+
+    // ---- fold counters ----
+    for (int off = 16; off > 0; off >>= 1) {
+        n_ext += __shfl_down_sync(kFull, n_ext, off);
+        n_sh += __shfl_down_sync(kFull, n_sh, off);
+        n_invalid += __shfl_down_sync(kFull, n_invalid, off);
+    }
+    if (lane == 0) {
+        if (n_ext) atomicAdd(&c->ext_rays, n_ext);
+        if (n_sh) atomicAdd(&c->shadow_rays, n_sh);
+        if (n_invalid) atomicAdd(&c->invalid, n_invalid);
+    }
+}
+
+__global__ void wavefront_init(Pool P, int capacity) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        Control* c = P.ctl;
+        c->n_active = (unsigned)capacity;
+    }
+    if (i < capacity) {
+        P.list[0][i] = (uint32_t)i;
+        P.alive[i] = 0u;
+        P.unit[i] = make_int4(-1, 0, 0, 0);
+    }
+}
+
+// Control block -> the renderer's counters (one thread; runs after the persistent kernel).
+__global__ void wavefront_fold(const Control* c, DevCounters* out, int count_rays) {
+    if (count_rays) {
+        out->extension_rays += c->ext_rays;
+        out->shadow_rays += c->shadow_rays;
+    }
+    out->invalid_hits += c->invalid;
+    out->overflows += c->overflow;
+    for (int i = 0; i < 5; ++i) out->high_water[i] = max(out->high_water[i], c->high_water[i]);
+    if (c->err) out->error = kErrSpinTimeout;
+}
+
+template <class T>
+T* carve(char*& p, size_t n) {
+    T* r = reinterpret_cast<T*>(p);
+    p += (n * sizeof(T) + 255) & ~(size_t)255;
+    return r;
+}
+
+size_t pool_bytes(int cap, Pool* out, char* base) {
+    char* p = base;
+    Pool P;
+    P.ray_o = carve<float4>(p, cap);
+    P.ray_d = carve<float4>(p, cap);
+    P.thr = carve<float4>(p, cap);
+    P.rad = carve<float4>(p, cap);
+    P.key = carve<uint2>(p, cap);
+    P.unit = carve<int4>(p, cap);
+    P.acc = carve<float4>(p, cap);
+    P.acc2 = carve<float>(p, cap);
+    P.hit = carve<float4>(p, cap);
+    P.surf_p = carve<float4>(p, cap);
+    P.surf_n = carve<float4>(p, cap);
+    P.alive = carve<uint32_t>(p, cap);
+    P.list[0] = carve<uint32_t>(p, cap);
+    P.list[1] = carve<uint32_t>(p, cap);
+    for (int q = 0; q < 4; ++q) P.queue[q] = carve<uint32_t>(p, cap);
+    P.sh_dir = carve<float4>(p, cap);
+    P.sh_c = carve<float4>(p, cap);
+    P.status = carve<unsigned long long>(p, (size_t)cap / kWfBlock + 2);
+    P.ctl = carve<Control>(p, 1);
+    if (out) *out = P;
+    return (size_t)(p - base);
+}
+
+}  // namespace
+
+struct WavefrontEngine::State {
+    Pool pool{};
+    float* lbuf = nullptr;
+    size_t lbuf_floats = 0;
+    int grid = 0;
+};
 
 WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixels_(pixels), cfg_(cfg) {
-    throw Error(WFB_ERR_UNSUPPORTED, "wavefront mode is not built yet");
+    if (pixels <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "wavefront needs at least one pixel");
+    int cap = cfg.paths_in_flight > 0 ? cfg.paths_in_flight : (1 << 20);
+    if (cap > pixels * 64) cap = pixels * 64;  // never more slots than units can use
+    if (cap < 32) cap = 32;
+    capacity_ = cap;
+    state_ = std::make_unique<State>();
+    const size_t bytes = pool_bytes(cap, nullptr, nullptr);
+    cuda_check(cudaMalloc(&arena_, bytes), "cudaMalloc wavefront pool");
+    bytes_ = bytes;
+    pool_bytes(cap, &state_->pool, static_cast<char*>(arena_));
+    int dev = 0, sms = 0, occ = 0, coop = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cooperative attribute");
+    if (!coop) throw Error(WFB_ERR_UNSUPPORTED, "device does not support cooperative launches");
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wavefront_persistent, kWfBlock, 0), "occupancy");
+    if (occ < 1) throw Error(WFB_ERR_UNSUPPORTED, "wavefront kernel does not fit on an SM");
+    state_->grid = sms * occ;
 }
 
 WavefrontEngine::~WavefrontEngine() {
+    if (state_ && state_->lbuf) cudaFree(state_->lbuf);
     if (arena_) cudaFree(arena_);
 }
 
-void WavefrontEngine::run(const DevScene&, const DevFilm&, DevCounters*, const PassParams&, wf::StageTimes*,
-                          cudaStream_t) {
-    throw Error(WFB_ERR_UNSUPPORTED, "wavefront mode is not built yet");
+uint64_t WavefrontEngine::bytes() const { return bytes_ + (state_ ? state_->lbuf_floats * sizeof(float) : 0); }
+
+void WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
+                          wf::StageTimes* stages, cudaStream_t stream) {
+    if (p.sample_count <= 0 || film.pixels <= 0) return;
+    State& st = *state_;
+    WfArgs a;
+    a.s = s;
+    a.film = film;
+    a.pool = st.pool;
+    a.capacity = capacity_;
+    a.pixels = film.pixels;
+    a.first_sample = p.first_sample;
+    a.sample_count = p.sample_count;
+    // Enough units to fill the pool: split a pixel's samples when pixels < slots.
+    int chunks = 1;
+    if (film.pixels < capacity_) chunks = std::min(p.sample_count, (capacity_ + film.pixels - 1) / film.pixels);
+    a.chunk = (p.sample_count + chunks - 1) / chunks;
+    a.chunks = (p.sample_count + a.chunk - 1) / a.chunk;
+    a.lbuf = nullptr;
+    if (a.chunks > 1) {
+        const size_t need = 3 * (size_t)film.pixels * (size_t)p.sample_count;
+        if (need > st.lbuf_floats) {
+            if (st.lbuf) cudaFree(st.lbuf);
+            st.lbuf = nullptr;
+            st.lbuf_floats = 0;
+            cuda_check(cudaMalloc(&st.lbuf, need * sizeof(float)), "cudaMalloc wavefront sample buffer");
+            st.lbuf_floats = need;
+        }
+        a.lbuf = st.lbuf;
+    }
+    a.seed = p.seed;
+    a.max_depth = p.max_depth;
+    a.qcap = (p.queue_capacity > 0 && p.queue_capacity < capacity_) ? (uint32_t)p.queue_capacity : (uint32_t)capacity_;
+    a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
+    a.split_shading = p.stage_timing ? 1 : 0;
+    Control* ctl = st.pool.ctl;
+    cuda_check(cudaMemsetAsync(ctl, 0, sizeof(Control), stream), "memset control");
+    cuda_check(cudaMemsetAsync(st.pool.status, 0, ((size_t)capacity_ / kWfBlock + 2) * sizeof(unsigned long long),
+                               stream), "memset status");
+    wavefront_init<<<(capacity_ + 255) / 256, 256, 0, stream>>>(st.pool, capacity_);
+    cuda_check(cudaGetLastError(), "wavefront init launch");
+    void* args[] = {&a};
+    cuda_check(cudaLaunchCooperativeKernel((const void*)wavefront_persistent, dim3(st.grid), dim3(kWfBlock), args, 0,
+                                           stream),
+               "wavefront cooperative launch");
+    if (a.chunks > 1) launch_film_commit(film, a.lbuf, p.sample_count, stream);
+    wavefront_fold<<<1, 1, 0, stream>>>(ctl, counters, p.count_rays ? 1 : 0);
+    cuda_check(cudaGetLastError(), "wavefront fold launch");
+    if (stages) {
+        unsigned long long ns[kStages];
+        cuda_check(cudaMemcpyAsync(ns, ctl->stage_ns, sizeof(ns), cudaMemcpyDeviceToHost, stream), "stage times");
+        cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+        stages->extend += ns[0] * 1e-6;
+        stages->classify += ns[1] * 1e-6;
+        stages->shade_lambert += ns[2] * 1e-6;
+        stages->shade_metal += ns[3] * 1e-6;
+        stages->shade_dielectric += ns[4] * 1e-6;
+        stages->shadow += ns[5] * 1e-6;
+        stages->compact += ns[6] * 1e-6;
+        stages->other += ns[7] * 1e-6;
+    }
 }
 
 }  // namespace wfb

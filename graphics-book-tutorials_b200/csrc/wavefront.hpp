@@ -1,15 +1,11 @@
 // Persistent-threads wavefront engine (wavefront.cu).
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <cuda_runtime.h>
 #include "engine.hpp"
 
 namespace wfb {
-
-struct WavefrontConfig {
-    int block = 256;           // threads per CTA
-    int paths_in_flight = 0;   // path-pool slots; 0: min(pixels, 1M)
-};
 
 class WavefrontEngine {
 public:
@@ -21,10 +17,12 @@ public:
     // Adds samples [p.first_sample, p.first_sample + p.sample_count) of every pixel to `film`.
     void run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
              wf::StageTimes* stages, cudaStream_t stream);
-    uint64_t bytes() const { return bytes_; }
+    uint64_t bytes() const;
     int capacity() const { return capacity_; }
 
 private:
+    struct State;
+    std::unique_ptr<State> state_;
     void* arena_ = nullptr;
     uint64_t bytes_ = 0;
     int capacity_ = 0;

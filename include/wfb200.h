@@ -155,6 +155,33 @@ int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */
 int wfb_renderer_destroy(wfb_renderer_t r);
 
+/* ---- queue primitives (WVM/src/gpu/queues.cuh:30-55) ------------------------------------------
+ * Device pointers in, stream-ordered, no host synchronisation. Status 1 (WFB_ERR_INVALID_ARGUMENT,
+ * the value of cudaErrorInvalidValue the reference returns) for n > capacity, with nothing enqueued.
+ * `stream` is a cudaStream_t (NULL = default stream). */
+typedef struct wfb_scan_workspace* wfb_scan_workspace_t;
+/* scan_workspace_create (WVM/src/gpu/queues.cu:99-111): look-back status for up to `capacity` items. */
+int wfb_scan_workspace_create(int capacity, wfb_scan_workspace_t* out);
+/* scan_workspace_destroy (WVM/src/gpu/queues.cu:113-119). */
+int wfb_scan_workspace_destroy(wfb_scan_workspace_t ws);
+/* scan_exclusive_u32 (WVM/src/gpu/queues.cu:175-196): out[i] = sum(in[0..i-1]), in may equal out,
+ * *d_total = sum (d_total may be NULL). Single pass (decoupled look-back). */
+int wfb_scan_exclusive_u32(const uint32_t* d_in, uint32_t* d_out, int n, uint32_t* d_total,
+                           wfb_scan_workspace_t ws, void* stream);
+/* compact_u32 (WVM/src/gpu/queues.cu:214-234): stable; out[k] = values[i] for the k-th i with
+ * flags[i] != 0, *d_count = number selected. d_scratch is accepted for signature compatibility and
+ * not used (the single-pass kernel needs no indicator array). */
+int wfb_compact_u32(const uint32_t* d_values, const uint32_t* d_flags, uint32_t* d_out, uint32_t* d_count,
+                    uint32_t* d_scratch, int n, wfb_scan_workspace_t ws, void* stream);
+/* test_queue_push (WVM/src/gpu/queues.cu:247-252): lanes i < n with flags[i] != 0 push i through the
+ * warp-aggregated queue_push with the given capacity; *d_counter and *d_overflow must be zeroed by
+ * the caller. Order inside the queue is unspecified. */
+int wfb_test_queue_push(const uint32_t* d_flags, int n, uint32_t* d_items, uint32_t capacity, uint32_t* d_counter,
+                        uint32_t* d_overflow, void* stream);
+/* Waits for `stream`; WFB_ERR_DEVICE_WAIT if a bounded look-back wait of this workspace gave up
+ * (no reference counterpart: the reference's scan has no device-side waits). */
+int wfb_scan_workspace_check(wfb_scan_workspace_t ws, void* stream);
+
 /* ---- allocation-free rendering ---------------------------------------------------------------
  * No counterpart in the reference. For callers that must not allocate device memory on their
  * render path: a host that owns all device memory through its own pool, a real-time loop where

@@ -106,6 +106,12 @@ def ref_lib() -> ctypes.CDLL:
         lib.ref_scene_view.argtypes = [vp, ctypes.POINTER(CScene)]
         lib.ref_scene_free.restype = None
         lib.ref_scene_free.argtypes = [vp]
+        lib.ref_scan.restype = i32
+        lib.ref_scan.argtypes = [vp, vp, i32, vp, i32]
+        lib.ref_compact.restype = i32
+        lib.ref_compact.argtypes = [vp, vp, vp, vp, vp, i32, i32]
+        lib.ref_queue_push.restype = i32
+        lib.ref_queue_push.argtypes = [vp, i32, vp, ctypes.c_uint32, vp, vp]
         _ref = lib
     return _ref
 

@@ -8,15 +8,34 @@
 //   ref_build_bvh     wf::build_bvh         (WVM/src/bvh_build.cpp:228)
 //   ref_scene_hash    wf::scene_hash        (WVM/src/scene.cpp:107)
 //   ref_make_scene    wf::make_scene        (WVM/src/scenes.cpp:29), exported as arrays
+//   ref_scan / ref_compact / ref_queue_push   wf::gpu queue primitives (WVM/src/gpu/queues.cu)
 // The scene struct below has the same field order as the engine's wfb_scene_desc.
 #include <cstdint>
 #include <cstring>
 #include <exception>
 #include <string>
 #include <vector>
+#include <cuda_runtime.h>
 #include "wf/bvh.hpp"
 #include "wf/renderer.hpp"
 #include "wf/scene.hpp"
+
+// Host-side interface of the reference queue primitives (WVM/src/gpu/queues.cuh:30-55), declared
+// here so this file stays host-only C++ (the header also carries device code).
+namespace wf::gpu {
+struct ScanWorkspace {
+    uint32_t* block_sums = nullptr;
+    int capacity = 0;
+};
+cudaError_t scan_workspace_create(ScanWorkspace* ws, int capacity);
+void scan_workspace_destroy(ScanWorkspace* ws);
+cudaError_t scan_exclusive_u32(const uint32_t* d_in, uint32_t* d_out, int n, uint32_t* d_total, ScanWorkspace& ws,
+                               cudaStream_t stream);
+cudaError_t compact_u32(const uint32_t* d_values, const uint32_t* d_flags, uint32_t* d_out, uint32_t* d_count,
+                        uint32_t* d_scratch, int n, ScanWorkspace& ws, cudaStream_t stream);
+cudaError_t test_queue_push(const uint32_t* d_flags, int n, uint32_t* d_items, uint32_t capacity, uint32_t* d_counter,
+                            uint32_t* d_overflow, cudaStream_t stream);
+}  // namespace wf::gpu
 
 namespace {
 
@@ -190,5 +209,34 @@ void ref_scene_view(const void* h, RefSceneDesc* d) {
 }
 
 void ref_scene_free(void* h) { delete static_cast<wf::Scene*>(h); }
+
+// Queue primitives on device pointers; each call makes its own workspace and synchronises.
+int ref_scan(const uint32_t* d_in, uint32_t* d_out, int n, uint32_t* d_total, int capacity) {
+    wf::gpu::ScanWorkspace ws;
+    cudaError_t e = wf::gpu::scan_workspace_create(&ws, capacity);
+    if (e != cudaSuccess) return (int)e;
+    e = wf::gpu::scan_exclusive_u32(d_in, d_out, n, d_total, ws, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    wf::gpu::scan_workspace_destroy(&ws);
+    return (int)e;
+}
+
+int ref_compact(const uint32_t* d_values, const uint32_t* d_flags, uint32_t* d_out, uint32_t* d_count,
+                uint32_t* d_scratch, int n, int capacity) {
+    wf::gpu::ScanWorkspace ws;
+    cudaError_t e = wf::gpu::scan_workspace_create(&ws, capacity);
+    if (e != cudaSuccess) return (int)e;
+    e = wf::gpu::compact_u32(d_values, d_flags, d_out, d_count, d_scratch, n, ws, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    wf::gpu::scan_workspace_destroy(&ws);
+    return (int)e;
+}
+
+int ref_queue_push(const uint32_t* d_flags, int n, uint32_t* d_items, uint32_t capacity, uint32_t* d_counter,
+                   uint32_t* d_overflow) {
+    cudaError_t e = wf::gpu::test_queue_push(d_flags, n, d_items, capacity, d_counter, d_overflow, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return (int)e;
+}
 
 }  // extern "C"

@@ -1,0 +1,128 @@
+"""Persistent wavefront on a B200: bit-for-bit against the reference's GPU arms and the engine's
+megakernel, pool-size independence, the queue-capacity test hook (counted overflows, clean next
+render; WVM/tests/catch/wavefront_failure.cu:92-134) and stage timing as pure observation."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_DIR, load_engine, load_oracle
+
+pytestmark = pytest.mark.gpu
+
+with open(os.path.join(GOLDEN_DIR, "golden.json")) as _f:
+    GOLDEN = json.load(_f)
+
+
+def _arrays(case):
+    g = GOLDEN[case]
+    kind, name = g["source"].split(":")
+    if kind == "engine":
+        return load_engine().Scene.generate(name, g["width"], g["height"], 1234, 16).export()
+    return load_oracle().ref_make_scene(name, g["width"], g["height"])
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def render(wfb, scene, mode, spp, seed, depth, configure=None, **kw):
+    r = wfb.GpuRenderer(scene, mode)
+    if configure:
+        r.configure(**configure)
+    st = wfb.RenderStats()
+    out = r.render(wfb.RenderParams(spp=spp, seed=seed, max_depth=depth, **kw), st)
+    return out, st, r
+
+
+@pytest.mark.parametrize("case", sorted(GOLDEN))
+def test_wavefront_bitwise_equals_reference_arms(wfb, ref, case):
+    g = GOLDEN[case]
+    arrays = _arrays(case)
+    out, st, _ = render(wfb, wfb.Scene.from_arrays(arrays), wfb.WAVEFRONT, g["spp"], g["seed"], g["max_depth"])
+    for mode in (0, 1):
+        rrgb, rvar, _ = ref.ref_render_gpu(arrays, mode, g["spp"], g["seed"], g["max_depth"])
+        assert np.array_equal(bits(out.rgb), bits(rrgb)), f"{case}: differs from reference arm {mode}"
+        assert np.array_equal(bits(out.lum_var), bits(rvar))
+    assert st.invalid_hits == 0 and st.queue_overflows == 0
+
+
+@pytest.mark.parametrize("pool", [32, 1000, 4096, 100000])
+def test_pool_size_never_changes_the_film(wfb, pool):
+    scene = wfb.Scene.generate("icospheres", 96, 54, 1234, 16)
+    mk, _, _ = render(wfb, scene, wfb.MEGAKERNEL, 6, 9, 8)
+    out, st, r = render(wfb, scene, wfb.WAVEFRONT, 6, 9, 8, configure={"paths_in_flight": pool})
+    assert np.array_equal(bits(out.rgb), bits(mk.rgb))
+    assert np.array_equal(bits(out.lum_var), bits(mk.lum_var))
+    assert 0 < st.queue_high_water[4] <= max(pool, 32)
+    assert all(0 <= v <= max(pool, 32) for v in st.queue_high_water[:4])
+
+
+def test_full_resolution_matches_megakernel_and_counts(wfb):
+    scene = wfb.Scene.generate("icospheres", 1280, 720, 1234, 16)
+    mk, smk, _ = render(wfb, scene, wfb.MEGAKERNEL, 2, 1234, 8, count_rays=True)
+    wv, swv, _ = render(wfb, scene, wfb.WAVEFRONT, 2, 1234, 8, count_rays=True)
+    assert np.array_equal(bits(wv.rgb), bits(mk.rgb))
+    assert swv.extension_rays == smk.extension_rays and swv.shadow_rays == smk.shadow_rays
+    assert swv.invalid_hits == 0 and swv.queue_overflows == 0
+
+
+def test_queue_capacity_hook_counts_overflows_and_recovers(wfb):
+    """Capacity far below the paths in flight: drops are counted, nothing faults, and the next
+    render without the hook is bit-exact again."""
+    scene = wfb.Scene.generate("icospheres", 64, 36, 1234, 16)
+    mk, _, _ = render(wfb, scene, wfb.MEGAKERNEL, 4, 5, 8)
+    r = wfb.GpuRenderer(scene, wfb.WAVEFRONT)
+    st = wfb.RenderStats()
+    capped = r.render(wfb.RenderParams(spp=4, seed=5, max_depth=8, queue_capacity=100), st)
+    assert st.queue_overflows > 0
+    assert np.isfinite(capped.rgb).all()
+    assert max(st.queue_high_water[:4]) <= 100
+    again = r.render(wfb.RenderParams(spp=4, seed=5, max_depth=8))
+    assert np.array_equal(bits(again.rgb), bits(mk.rgb))
+
+
+def test_capacity_equal_to_pool_never_overflows(wfb):
+    scene = wfb.Scene.generate("cornell36", 64, 36, 1234, 16)
+    r = wfb.GpuRenderer(scene, wfb.WAVEFRONT)
+    r.configure(paths_in_flight=2304)
+    st = wfb.RenderStats()
+    r.render(wfb.RenderParams(spp=4, seed=1, max_depth=8, queue_capacity=2304), st)
+    assert st.queue_overflows == 0
+
+
+def test_stage_timing_is_observation_only(wfb):
+    scene = wfb.Scene.generate("icospheres", 128, 72, 1234, 16)
+    plain, _, _ = render(wfb, scene, wfb.WAVEFRONT, 4, 3, 8)
+    timed, st, _ = render(wfb, scene, wfb.WAVEFRONT, 4, 3, 8, stage_timing=True)
+    assert np.array_equal(bits(plain.rgb), bits(timed.rgb))
+    assert st.stages["extend"] > 0 and st.stages["shadow"] > 0 and st.stages["compact"] > 0
+
+
+def test_progressive_equals_one_shot(wfb):
+    scene = wfb.Scene.generate("cornell36", 64, 36, 1234, 16)
+    r = wfb.GpuRenderer(scene, wfb.WAVEFRONT)
+    p = wfb.RenderParams(spp=8, seed=3, max_depth=8)
+    one = r.render(p)
+    r.reset()
+    r.run_passes(0, 3, p)
+    r.run_passes(3, 5, p)
+    assert np.array_equal(bits(one.rgb), bits(r.download(8).rgb))
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (33, 17), (31, 1), (1, 33)])
+def test_odd_sizes_match_reference(wfb, ref, w, h):
+    arrays = load_oracle().ref_make_scene("divergence", w, h)
+    out, _, _ = render(wfb, wfb.Scene.from_arrays(arrays), wfb.WAVEFRONT, 4, 7, 8)
+    rrgb, rvar, _ = ref.ref_render_gpu(arrays, 1, 4, 7, 8)
+    assert np.array_equal(bits(out.rgb), bits(rrgb))
+    assert np.array_equal(bits(out.lum_var), bits(rvar))
+
+
+def test_depth_zero_and_deep_paths(wfb, ref):
+    arrays = _arrays("ref_furnace_32x18")
+    for depth in (0, 1, 50):
+        out, _, _ = render(wfb, wfb.Scene.from_arrays(arrays), wfb.WAVEFRONT, 2, 7, depth)
+        rrgb, _, _ = ref.ref_render_gpu(arrays, 0, 2, 7, depth)
+        assert np.array_equal(bits(out.rgb), bits(rrgb)), depth
