@@ -450,3 +450,244 @@ def test_queue_push(d_flags: int, n: int, d_items: int, capacity: int, d_counter
     """test_queue_push (WVM/src/gpu/queues.cuh:53-54) on device pointers; returns the C status."""
     return load_library().wfb_test_queue_push(d_flags, n, d_items or None, capacity & 0xFFFFFFFF, d_counter,
                                               d_overflow, stream or None)
+
+
+# ---------------------------------------------------------------------------------------------
+# Batched rendering and the render server (no reference counterpart).
+
+class _CJobDesc(ctypes.Structure):
+    _fields_ = [("cam_position", ctypes.c_float * 3), ("cam_look_at", ctypes.c_float * 3),
+                ("cam_up", ctypes.c_float * 3), ("cam_vfov_deg", ctypes.c_float), ("width", ctypes.c_int),
+                ("height", ctypes.c_int), ("spp", ctypes.c_int), ("seed", ctypes.c_uint32),
+                ("max_depth", ctypes.c_int)]
+
+
+class _CServerConfig(ctypes.Structure):
+    _fields_ = [("budget_bytes", ctypes.c_uint64), ("max_jobs", ctypes.c_int), ("launch_target_ms", ctypes.c_double),
+                ("fixed_slice", ctypes.c_int), ("one_job_per_launch", ctypes.c_int), ("use_graph", ctypes.c_int),
+                ("block", ctypes.c_int), ("min_active", ctypes.c_int)]
+
+
+class _CServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("cancelled", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("launches", ctypes.c_uint64), ("samples_done", ctypes.c_uint64),
+                ("busy_ms", ctypes.c_double), ("wall_s", ctypes.c_double), ("p50_ms", ctypes.c_double),
+                ("p95_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("bytes_in_use", ctypes.c_uint64), ("peak_bytes", ctypes.c_uint64),
+                ("queued", ctypes.c_int), ("active", ctypes.c_int)]
+
+
+JOB_QUEUED, JOB_ACTIVE, JOB_DONE, JOB_CANCELLED, JOB_FAILED = range(5)
+
+
+@dataclass
+class JobDesc:
+    """One render job: camera, resolution, samples, seed, depth (scene passed separately)."""
+    cam_position: tuple
+    cam_look_at: tuple
+    cam_up: tuple = (0.0, 1.0, 0.0)
+    cam_vfov_deg: float = 50.0
+    width: int = 256
+    height: int = 256
+    spp: int = 1
+    seed: int = 1
+    max_depth: int = 8
+
+    def _c(self) -> _CJobDesc:
+        f3 = ctypes.c_float * 3
+        return _CJobDesc(f3(*self.cam_position), f3(*self.cam_look_at), f3(*self.cam_up), float(self.cam_vfov_deg),
+                         int(self.width), int(self.height), int(self.spp), int(self.seed) & 0xFFFFFFFF,
+                         int(self.max_depth))
+
+
+def _bind_batch_server(lib):
+    vp, i32, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64
+    jd = ctypes.POINTER(_CJobDesc)
+    sig = {
+        "wfb_batch_create": (i32, [i32, i32, i32, i32, ctypes.POINTER(vp)]),
+        "wfb_batch_add": (i32, [vp, vp, jd, ctypes.POINTER(i32)]),
+        "wfb_batch_clear": (i32, [vp]),
+        "wfb_batch_run": (i32, [vp, i32, ctypes.POINTER(_CRenderStats)]),
+        "wfb_batch_download": (i32, [vp, i32, vp, vp]),
+        "wfb_batch_download_sums": (i32, [vp, i32, vp, vp, vp]),
+        "wfb_batch_destroy": (i32, [vp]),
+        "wfb_server_create": (i32, [ctypes.POINTER(_CServerConfig), ctypes.POINTER(vp)]),
+        "wfb_server_submit": (i32, [vp, vp, jd, ctypes.POINTER(u64)]),
+        "wfb_server_poll": (i32, [vp, u64, ctypes.POINTER(i32)]),
+        "wfb_server_wait": (i32, [vp, u64, i32]),
+        "wfb_server_result": (i32, [vp, u64, vp, vp, ctypes.POINTER(ctypes.c_double)]),
+        "wfb_server_cancel": (i32, [vp, u64]),
+        "wfb_server_stats_get": (i32, [vp, ctypes.POINTER(_CServerStats)]),
+        "wfb_server_reset_stats": (i32, [vp]),
+        "wfb_server_destroy": (i32, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+class Batch:
+    """Many jobs in one persistent launch (wfb_batch_*); every job's film equals its solo render."""
+
+    def __init__(self, max_jobs: int = 64, use_graph: bool = True, block: int = 0, min_active: int = 0):
+        lib = _bind_batch_server(load_library())
+        h = ctypes.c_void_p()
+        _check(lib.wfb_batch_create(int(max_jobs), int(bool(use_graph)), int(block), int(min_active), ctypes.byref(h)))
+        self._h = h
+        self._jobs = []
+        self._scenes = []
+
+    def add(self, scene: Scene, job: JobDesc) -> int:
+        jid = ctypes.c_int()
+        _check(load_library().wfb_batch_add(self._h, scene.handle, ctypes.byref(job._c()), ctypes.byref(jid)))
+        self._jobs.append(job)
+        self._scenes.append(scene)
+        return jid.value
+
+    def clear(self) -> None:
+        _check(load_library().wfb_batch_clear(self._h))
+        self._jobs.clear()
+        self._scenes.clear()
+
+    def run(self, count_rays: bool = False) -> RenderStats:
+        cs = _CRenderStats()
+        _check(load_library().wfb_batch_run(self._h, int(bool(count_rays)), ctypes.byref(cs)))
+        return RenderStats._from_c(cs)
+
+    def download(self, job_id: int) -> RenderResult:
+        j = self._jobs[job_id]
+        rgb = np.empty((j.height, j.width, 3), np.float32)
+        var = np.empty((j.height, j.width), np.float32)
+        _check(load_library().wfb_batch_download(self._h, job_id, _ptr(rgb), _ptr(var)))
+        return RenderResult(j.width, j.height, j.spp, rgb, var)
+
+    def download_sums(self, job_id: int):
+        j = self._jobs[job_id]
+        rgb = np.empty((j.height, j.width, 3), np.float32)
+        lum = np.empty((j.height, j.width), np.float32)
+        lum2 = np.empty((j.height, j.width), np.float32)
+        _check(load_library().wfb_batch_download_sums(self._h, job_id, _ptr(rgb), _ptr(lum), _ptr(lum2)))
+        return rgb, lum, lum2
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            load_library().wfb_batch_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching render server (wfb_server_*). Thread-safe submit/wait/result."""
+
+    def __init__(self, budget_bytes: int = 0, max_jobs: int = 0, launch_target_ms: float = 0.0,
+                 fixed_slice: int = 0, one_job_per_launch: bool = False, use_graph: bool = True, block: int = 0,
+                 min_active: int = 0):
+        lib = _bind_batch_server(load_library())
+        cfg = _CServerConfig(int(budget_bytes), int(max_jobs), float(launch_target_ms), int(fixed_slice),
+                             int(bool(one_job_per_launch)), int(bool(use_graph)), int(block), int(min_active))
+        h = ctypes.c_void_p()
+        _check(lib.wfb_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._jobs = {}
+        self._scenes = {}
+
+    def submit(self, scene: Scene, job: JobDesc) -> int:
+        t = ctypes.c_uint64()
+        _check(load_library().wfb_server_submit(self._h, scene.handle, ctypes.byref(job._c()), ctypes.byref(t)))
+        self._jobs[t.value] = job
+        self._scenes[t.value] = scene
+        return t.value
+
+    def poll(self, ticket: int) -> int:
+        st = ctypes.c_int()
+        _check(load_library().wfb_server_poll(self._h, ticket, ctypes.byref(st)))
+        return st.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> bool:
+        rc = load_library().wfb_server_wait(self._h, ticket, int(timeout_ms))
+        if rc == ERR_TIMEOUT:
+            return False
+        _check(rc)
+        return True
+
+    def result(self, ticket: int):
+        j = self._jobs.pop(ticket)
+        self._scenes.pop(ticket, None)
+        rgb = np.empty((j.height, j.width, 3), np.float32)
+        var = np.empty((j.height, j.width), np.float32)
+        lat = ctypes.c_double()
+        _check(load_library().wfb_server_result(self._h, ticket, _ptr(rgb), _ptr(var), ctypes.byref(lat)))
+        return RenderResult(j.width, j.height, j.spp, rgb, var), lat.value
+
+    def cancel(self, ticket: int) -> None:
+        _check(load_library().wfb_server_cancel(self._h, ticket))
+
+    def stats(self) -> dict:
+        s = _CServerStats()
+        _check(load_library().wfb_server_stats_get(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in _CServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        _check(load_library().wfb_server_reset_stats(self._h))
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            load_library().wfb_server_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+MIX_SCENES = ("cornell36", "icospheres", "heightfield")
+MIX_RESOLUTIONS = ((256, 256), (640, 360), (1280, 720), (1920, 1080))
+MIX_SPP = (1, 4, 16, 64)
+MIX_DEPTHS = (4, 8)
+
+
+def orbit_camera(default_position, look_at, azimuth_deg: float, elevation_deg: float):
+    """Camera on the orbit of the scene's default camera around its look-at point (float32)."""
+    p = np.asarray(default_position, np.float32)
+    t = np.asarray(look_at, np.float32)
+    dist = np.float32(np.sqrt(np.float32(((p - t) ** 2).sum())))
+    az, el = np.radians(np.float32(azimuth_deg)), np.radians(np.float32(elevation_deg))
+    d = np.array([np.cos(el) * np.sin(az), np.sin(el), np.cos(el) * np.cos(az)], np.float32)
+    return tuple(float(v) for v in (t + d * dist))
+
+
+def job_mix(n: int = 64, seed: int = 1234):
+    """The batched/served job distribution: n jobs with scene, resolution, spp and depth drawn
+    uniformly from the sets above, seeds 1..n, orbit cameras at azimuth U(0, 360) and elevation
+    U(10, 40) degrees. PRNG: numpy PCG64 seeded with `seed`; draws in this order per job: scene,
+    resolution, spp, depth, azimuth, elevation. Returns a list of plain dicts."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(n):
+        scene = MIX_SCENES[int(rng.integers(len(MIX_SCENES)))]
+        w, h = MIX_RESOLUTIONS[int(rng.integers(len(MIX_RESOLUTIONS)))]
+        spp = MIX_SPP[int(rng.integers(len(MIX_SPP)))]
+        depth = MIX_DEPTHS[int(rng.integers(len(MIX_DEPTHS)))]
+        az = float(rng.uniform(0.0, 360.0))
+        el = float(rng.uniform(10.0, 40.0))
+        jobs.append({"scene": scene, "width": w, "height": h, "spp": spp, "max_depth": depth, "seed": i + 1,
+                     "azimuth": round(az, 4), "elevation": round(el, 4)})
+    return jobs
+
+
+def mix_job_desc(job: dict, scene: Scene) -> JobDesc:
+    """JobDesc of a job_mix entry on `scene` (orbit camera around the scene's default camera)."""
+    inf = scene.info()
+    pos = orbit_camera(list(inf.cam_position), list(inf.cam_look_at), job["azimuth"], job["elevation"])
+    return JobDesc(cam_position=pos, cam_look_at=tuple(inf.cam_look_at), cam_up=tuple(inf.cam_up),
+                   cam_vfov_deg=inf.cam_vfov_deg, width=job["width"], height=job["height"], spp=job["spp"],
+                   seed=job["seed"], max_depth=job["max_depth"])

@@ -7,6 +7,7 @@
 #include "engine.hpp"
 #include "noalloc.hpp"
 #include "queues.hpp"
+#include "server.hpp"
 #include "scene_gen.hpp"
 #include "../../include/wfb200.h"
 
@@ -28,6 +29,33 @@ struct wfb_renderer {
 struct wfb_scan_workspace {
     std::unique_ptr<wfb::ScanWorkspace> ws;
 };
+
+struct wfb_batch {
+    std::unique_ptr<wfb::BatchRenderer> b;
+    std::vector<std::shared_ptr<wfb::ResidentScene>> scenes;  // keeps job scenes resident
+};
+
+struct wfb_server {
+    std::unique_ptr<wfb::Server> s;
+};
+
+namespace {
+wfb::JobSpec job_spec(wfb_scene_t scene, const wfb_job_desc* d) {
+    wfb::JobSpec j;
+    j.scene = scene->get_resident();
+    j.camera.position = wf::Vec3{d->cam_position[0], d->cam_position[1], d->cam_position[2]};
+    j.camera.look_at = wf::Vec3{d->cam_look_at[0], d->cam_look_at[1], d->cam_look_at[2]};
+    j.camera.up = wf::Vec3{d->cam_up[0], d->cam_up[1], d->cam_up[2]};
+    j.camera.vfov_deg = d->cam_vfov_deg;
+    j.width = d->width;
+    j.height = d->height;
+    j.first_sample = 0;
+    j.sample_count = d->spp;
+    j.seed = d->seed;
+    j.max_depth = d->max_depth;
+    return j;
+}
+}  // namespace
 
 namespace {
 
@@ -311,6 +339,158 @@ int wfb_renderer_height(wfb_renderer_t r) { return r ? r->r->height() : 0; }
 
 int wfb_renderer_destroy(wfb_renderer_t r) {
     delete r;
+    return WFB_OK;
+}
+
+int wfb_batch_create(int max_jobs, int use_graph, int block, int min_active, wfb_batch_t* out) {
+    return guarded([&] {
+        need(out != nullptr, "null argument");
+        wfb::MegakernelConfig cfg;
+        if (block > 0) cfg.block = block;
+        if (min_active > 0) cfg.min_active = min_active;
+        need(cfg.block == 64 || cfg.block == 128 || cfg.block == 256, "block must be 64, 128 or 256");
+        need(cfg.min_active <= 32, "min_active must be in 1..32");
+        auto b = std::make_unique<wfb_batch>();
+        b->b = std::make_unique<wfb::BatchRenderer>(max_jobs, cfg, use_graph != 0);
+        *out = b.release();
+    });
+}
+
+int wfb_batch_add(wfb_batch_t b, wfb_scene_t scene, const wfb_job_desc* job, int* job_id) {
+    return guarded([&] {
+        need(b && scene && job, "null argument");
+        if (scene->host.nodes.empty()) throw wfb::Error(WFB_ERR_NOT_FINALIZED, "Scene not finalized (no BVH nodes)");
+        wfb::JobSpec j = job_spec(scene, job);
+        const int id = b->b->add(j);
+        b->scenes.push_back(j.scene);
+        if (job_id) *job_id = id;
+    });
+}
+
+int wfb_batch_clear(wfb_batch_t b) {
+    return guarded([&] {
+        need(b != nullptr, "null batch");
+        b->b->clear();
+        b->scenes.clear();
+    });
+}
+
+int wfb_batch_run(wfb_batch_t b, int count_rays, wfb_render_stats* stats) {
+    return guarded([&] {
+        need(b != nullptr, "null batch");
+        wf::RenderStats st{};
+        b->b->run(count_rays != 0, &st);
+        if (stats) to_c_stats(st, stats);
+    });
+}
+
+int wfb_batch_download(wfb_batch_t b, int job_id, float* rgb, float* lum_var) {
+    return guarded([&] {
+        need(b != nullptr, "null batch");
+        b->b->download(job_id, b->b->job(job_id).sample_count, rgb, lum_var);
+    });
+}
+
+int wfb_batch_download_sums(wfb_batch_t b, int job_id, float* rgb_sum, float* lum_sum, float* lum2_sum) {
+    return guarded([&] {
+        need(b != nullptr, "null batch");
+        b->b->download_sums(job_id, rgb_sum, lum_sum, lum2_sum);
+    });
+}
+
+int wfb_batch_destroy(wfb_batch_t b) {
+    delete b;
+    return WFB_OK;
+}
+
+int wfb_server_create(const wfb_server_config* c, wfb_server_t* out) {
+    return guarded([&] {
+        need(c && out, "null argument");
+        wfb::ServerConfig cfg;
+        if (c->budget_bytes > 0) cfg.budget_bytes = c->budget_bytes;
+        if (c->max_jobs > 0) cfg.max_jobs = c->max_jobs;
+        if (c->launch_target_ms > 0) cfg.launch_target_ms = c->launch_target_ms;
+        cfg.fixed_slice = c->fixed_slice;
+        cfg.one_job_per_launch = c->one_job_per_launch != 0;
+        cfg.use_graph = c->use_graph != 0;
+        if (c->block > 0) cfg.cfg.block = c->block;
+        if (c->min_active > 0) cfg.cfg.min_active = c->min_active;
+        need(cfg.cfg.block == 64 || cfg.cfg.block == 128 || cfg.cfg.block == 256, "block must be 64, 128 or 256");
+        auto s = std::make_unique<wfb_server>();
+        s->s = std::make_unique<wfb::Server>(cfg);
+        *out = s.release();
+    });
+}
+
+int wfb_server_submit(wfb_server_t s, wfb_scene_t scene, const wfb_job_desc* job, uint64_t* ticket) {
+    return guarded([&] {
+        need(s && scene && job && ticket, "null argument");
+        if (scene->host.nodes.empty()) throw wfb::Error(WFB_ERR_NOT_FINALIZED, "Scene not finalized (no BVH nodes)");
+        *ticket = s->s->submit(job_spec(scene, job));
+    });
+}
+
+int wfb_server_poll(wfb_server_t s, uint64_t ticket, int* state) {
+    return guarded([&] {
+        need(s && state, "null argument");
+        *state = s->s->state(ticket);
+    });
+}
+
+int wfb_server_wait(wfb_server_t s, uint64_t ticket, int timeout_ms) {
+    return guarded([&] {
+        need(s != nullptr, "null server");
+        if (!s->s->wait(ticket, timeout_ms)) throw wfb::Error(WFB_ERR_TIMEOUT, "job not finished before the timeout");
+    });
+}
+
+int wfb_server_result(wfb_server_t s, uint64_t ticket, float* rgb, float* lum_var, double* latency_ms) {
+    return guarded([&] {
+        need(s != nullptr, "null server");
+        s->s->result(ticket, rgb, lum_var, latency_ms);
+    });
+}
+
+int wfb_server_cancel(wfb_server_t s, uint64_t ticket) {
+    return guarded([&] {
+        need(s != nullptr, "null server");
+        if (!s->s->cancel(ticket)) throw wfb::Error(WFB_ERR_INVALID_ARGUMENT, "job is finished or unknown");
+    });
+}
+
+int wfb_server_stats_get(wfb_server_t s, wfb_server_stats* out) {
+    return guarded([&] {
+        need(s && out, "null argument");
+        const wfb::ServerStats st = s->s->stats();
+        out->submitted = st.submitted;
+        out->completed = st.completed;
+        out->cancelled = st.cancelled;
+        out->failed = st.failed;
+        out->launches = st.launches;
+        out->samples_done = st.samples_done;
+        out->busy_ms = st.busy_ms;
+        out->wall_s = st.wall_s;
+        out->p50_ms = st.p50_ms;
+        out->p95_ms = st.p95_ms;
+        out->p99_ms = st.p99_ms;
+        out->mean_ms = st.mean_ms;
+        out->max_ms = st.max_ms;
+        out->bytes_in_use = st.bytes_in_use;
+        out->peak_bytes = st.peak_bytes;
+        out->queued = st.queued;
+        out->active = st.active;
+    });
+}
+
+int wfb_server_reset_stats(wfb_server_t s) {
+    return guarded([&] {
+        need(s != nullptr, "null server");
+        s->s->reset_stats();
+    });
+}
+
+int wfb_server_destroy(wfb_server_t s) {
+    delete s;
     return WFB_OK;
 }
 

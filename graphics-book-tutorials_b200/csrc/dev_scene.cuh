@@ -175,6 +175,81 @@ __device__ __forceinline__ bool intersect_dev(const DevScene& s, wf::Ray r, wf::
     return h->prim >= 0;
 }
 
+// A ray being traversed by the resumable form of the traversal below.
+struct TravRay {
+    wf::Vec3 o, d, inv_d;
+    float tmin;
+};
+
+// One step of the stackless skip-link traversal, resumable between calls: the whole state is the
+// next node index `node` (-1 when done) and the best hit `h` (h.t is the current tmax). Visiting
+// order, box and primitive arithmetic and the strictly-nearer rule are intersect_dev's, so running
+// steps until node < 0 gives bit-identical hits. `anyhit` ends the query at the first hit.
+__device__ __forceinline__ void traversal_step(const float4* __restrict__ nodes, const float4* __restrict__ prims,
+                                               int n_nodes, int n_spheres, const TravRay& ray, bool anyhit,
+                                               int& node, wf::HitRecord& h) {
+    const float4 na = __ldg(&nodes[2 * node]);
+    const float4 nb = __ldg(&nodes[2 * node + 1]);
+    const int skip = __float_as_int(na.w);
+    wf::Ray r;
+    r.o = ray.o;
+    r.d = ray.d;
+    r.tmin = ray.tmin;
+    r.tmax = h.t;
+    if (!wf::hit_box(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, r.o, ray.inv_d, r.tmin, r.tmax)) {
+        node = skip;
+    } else {
+        const int leaf = __float_as_int(nb.w);
+        if (leaf < 0) {
+            node = node + 1;
+        } else {
+            node = skip;
+            const int count = leaf & kLeafCountMask;
+            const float4* rec = prims + 3 * (leaf >> kLeafCountBits);
+            for (int i = 0; i < count; ++i, rec += 3) {
+                const float4 q0 = __ldg(rec);
+                const float4 q1 = __ldg(rec + 1);
+                const int p = __float_as_int(q0.w);
+                float t, u = 0.0f, v = 0.0f;
+                bool hit;
+                if (p < n_spheres) {
+                    hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
+                } else {
+                    const float4 q2 = __ldg(rec + 2);
+                    hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
+                                                wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
+                }
+                if (hit) {
+                    r.tmax = t;
+                    h.t = t;
+                    h.prim = p;
+                    h.u = u;
+                    h.v = v;
+                    if (anyhit) {
+                        node = -1;
+                        return;
+                    }
+                }
+            }
+        }
+    }
+    if (node >= n_nodes) node = -1;
+}
+
+// intersect() prologue (WVM/include/wf/bvh.hpp:92-94): the ray's traversal state before step 0.
+__device__ __forceinline__ void traversal_begin(int n_nodes, wf::Vec3 o, wf::Vec3 d, float tmin, float tmax,
+                                                TravRay* ray, int* node, wf::HitRecord* h) {
+    ray->o = o;
+    ray->d = d;
+    ray->tmin = tmin;
+    ray->inv_d = wf::Vec3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    h->t = tmax;
+    h->prim = -1;
+    h->u = 0.0f;
+    h->v = 0.0f;
+    *node = n_nodes > 0 ? 0 : -1;
+}
+
 // Validity check applied after every closest-hit query (WVM/src/gpu/engine.cuh:44-48).
 __device__ __forceinline__ bool hit_is_valid(const DevScene& s, const wf::HitRecord& h) {
     if (h.prim < 0) return true;

@@ -69,6 +69,35 @@ void launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* coun
 // film sums in ascending sample order (megakernel.cu).
 void launch_film_commit(const DevFilm& film, const float* lbuf, int count, cudaStream_t stream);
 
+// One render job inside a launch: scene + camera (in `s`), film, sample range, split mode.
+// Its work units are [unit_begin, unit_begin + units) of the launch; unit u covers pixel
+// (u - unit_begin) mod pixels and chunk (u - unit_begin) div pixels of `chunk` samples.
+struct JobDesc {
+    DevScene s;
+    DevFilm film;
+    float* lbuf;  // chunks > 1: 3 floats per (pixel, sample - first_sample)
+    int first_sample, sample_count, chunk, chunks;
+    uint32_t seed;
+    int max_depth;
+    unsigned unit_begin, units;
+};
+
+// Device-resident size of a batch launch, so a captured graph can be replayed for any batch.
+struct BatchHeader {
+    unsigned n_jobs;
+    unsigned total_units;
+    unsigned pad[62];
+};
+
+JobDesc make_job(const DevScene& s, const DevFilm& film, float* lbuf, int first_sample, int sample_count,
+                 int chunks, uint32_t seed, int max_depth);
+// Persistent megakernel over a device job table (unit_begin must be the running sum of units)
+// followed by the split-mode commits of its jobs; max_jobs bounds the job count of any batch
+// replayed through the same launch. Stream-ordered, no host synchronisation, capturable.
+void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, int max_jobs, DevCounters* counters,
+                             unsigned int* work_counter, bool count_rays, const MegakernelConfig& cfg,
+                             cudaStream_t stream);
+
 // ---- wavefront (wavefront.cu) ----
 struct WavefrontConfig {
     int paths_in_flight = 0;  // path-pool slots; 0: 1M (capped at 64 x pixels)

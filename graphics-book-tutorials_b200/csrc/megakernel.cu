@@ -1,4 +1,5 @@
-// Persistent megakernel: one lane per path, register-resident state, one launch per render.
+// Persistent megakernel: one lane per path, register-resident state, one launch per render -- or
+// per batch of render jobs.
 //
 // Replaces megakernel_kernel / run_megakernel_pass (WVM/src/gpu/megakernel.cu:11-104), which
 // launches one thread per pixel per sample, traces each path to completion and synchronises the
@@ -6,26 +7,29 @@
 //
 //  * Persistent threads: the grid is the set of CTAs resident at once; work units are handed out
 //    by a global counter with warp-aggregated fetches (one atomic per warp per refill).
-//  * Resumable traversal: the stackless skip-link traversal state of a ray is just the next node
-//    index plus the best hit so far, so it survives across loop iterations. A warp keeps stepping
-//    the traversal of all its lanes while at least `min_active` lanes are still traversing; only
-//    then does it run the shading code, for exactly the lanes whose ray has finished, and gives
-//    them their next ray (the extension ray, the pending shadow ray of a Lambertian bounce, or
-//    the camera ray of the next sample). Lanes that are mid-traversal keep their state. This is
-//    the "dynamic ray fetch" of Aila and Laine (HPG 2009) adapted to one-lane-per-path shading.
-//  * Film order: a work unit is one pixel and a run of its samples in ascending order. In direct
-//    mode a unit covers all samples of the pixel and the lane adds every finished path to register
-//    copies of the pixel's film sums (film_add order of WVM/src/gpu/engine.cuh:25-32), writing the
-//    film once. In split mode (images with fewer pixels than resident lanes) a pixel's samples are
-//    cut into chunks handed to different lanes; each path's radiance goes to its (pixel, sample)
-//    slot of a scratch buffer and a second kernel adds the slots to the film in sample order.
-//    Both modes produce bit-identical films.
+//  * Jobs: a work unit belongs to one job (scene, camera, resolution, seed, depth, film). A single
+//    render is a batch of one job passed in parameter space; a batch of many jobs is a device-side
+//    job table whose units are numbered consecutively, so paths of different jobs share one launch
+//    and the tail of one job overlaps the others. Per-job pixel ids stay job-local (the RNG key
+//    uses py * width + px of the job, WVM/include/wf/path_core.hpp:74), so a job renders the same
+//    bits alone and inside any batch.
+//  * Resumable traversal: a ray's traversal state is the next node index plus the best hit
+//    (traversal_step, dev_scene.cuh). A warp keeps stepping all traversing lanes while at least
+//    `min_active` lanes traverse; only then does it shade the lanes whose ray finished and give
+//    them their next ray (extension, the pending shadow ray of a Lambertian bounce, or the camera
+//    ray of the next sample) -- the "dynamic ray fetch" of Aila and Laine (HPG 2009) with
+//    one-lane-per-path shading.
+//  * Film order: a unit is one pixel and a run of its samples in ascending order. Direct mode: a
+//    unit covers all samples of the pixel; the lane adds every finished path to register copies of
+//    the film sums (film_add order, WVM/src/gpu/engine.cuh:25-32). Split mode (a job with fewer
+//    pixels than resident lanes): a pixel's samples are cut into chunks on different lanes; each
+//    path's radiance goes to its (pixel, sample) slot of a buffer and film_commit adds the slots
+//    in sample order. Both produce bit-identical films.
 //  * The shadow ray of a Lambertian bounce starts at the next extension ray's origin
-//    (p + n * eps, WVM/include/wf/path_core.hpp:197,210,226); only its direction, tmax and
+//    (p + n * eps, WVM/include/wf/path_core.hpp:197,210,226); only direction, tmax and
 //    contribution are kept.
 //  * Ray counters live in registers and are folded with one atomic per warp at exit.
-// Every per-path float operation is the reference's (see wf/path_core.hpp), so the film is
-// bit-identical to the reference arms for the same scene arrays and seed.
+#include <algorithm>
 #include "engine.hpp"
 #include "../../include/wfb200.h"
 
@@ -35,30 +39,28 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 
 struct MkArgs {
-    DevScene s;
-    DevFilm film;
+    JobDesc job0;              // single-job launch
+    const JobDesc* jobs;       // batch launch: device job table
+    const BatchHeader* hdr;    // batch launch: job count and total units (device)
     DevCounters* counters;
     unsigned int* work;
-    float* lbuf;        // split mode: radiance per (pixel, sample - first), 3 floats each
-    int pixels;
-    int first_sample;
-    int sample_count;
-    int chunk;          // samples per work unit (== sample_count in direct mode)
-    int chunks;         // work units per pixel
-    uint32_t seed;
-    int max_depth;
     int count_rays;
-    int min_active;     // keep traversing while at least this many lanes of the warp traverse
+    int min_active;
 };
 
-template <int BLOCK>
+template <bool MULTI>
+__device__ __forceinline__ const JobDesc& job_at(const MkArgs& a, int j) {
+    return MULTI ? a.jobs[j] : a.job0;
+}
+
+template <int BLOCK, bool MULTI>
 __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
-    const DevScene& s = a.s;
     const int lane = threadIdx.x & 31;
-    const bool split = a.chunks > 1;
-    const unsigned total_units = (unsigned)a.pixels * (unsigned)a.chunks;
+    const unsigned total_units = MULTI ? a.hdr->total_units : a.job0.units;
+    const int n_jobs = MULTI ? (int)a.hdr->n_jobs : 1;
 
     // ---- per-lane work and path state ----
+    int job = 0;
     int pixel = -1, px = 0, py = 0, sample = 0, s_end = 0;
     bool out_of_work = false;
     wf::PathState ps{};
@@ -66,27 +68,22 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
     bool shadow_ray = false, alive_after_shadow = false;
     wf::Vec3 sh_dir{0.f, 0.f, 0.f}, sh_contrib{0.f, 0.f, 0.f};
     float sh_tmax = 0.f;
-    // ---- traversal state of the lane's current ray ----
-    int node = -1;  // next node to visit; -1: no ray in flight
-    wf::Vec3 rd{0.f, 0.f, 1.f}, inv_d{0.f, 0.f, 1.f};
-    float r_tmin = 0.f;
+    // ---- traversal state of the lane's current ray (+ the job's BVH, cached) ----
+    int node = -1;
+    TravRay ray;
     wf::HitRecord h;
     h.t = 0.f;
     h.prim = -1;
     h.u = h.v = 0.f;
+    const float4* jnodes = a.job0.s.nodes;
+    const float4* jprims = a.job0.s.prims;
+    int jn_nodes = a.job0.s.n_nodes, jn_spheres = a.job0.s.n_spheres;
     unsigned long long n_ext = 0, n_shadow = 0;
     unsigned int n_invalid = 0;
 
     auto start_ray = [&]() {
-        // intersect() prologue (WVM/include/wf/bvh.hpp:92-94) for the extension or shadow ray.
-        rd = shadow_ray ? sh_dir : ps.ray.d;
-        r_tmin = shadow_ray ? wf::kRayEps : ps.ray.tmin;
-        h.t = shadow_ray ? sh_tmax : ps.ray.tmax;
-        h.prim = -1;
-        h.u = 0.0f;
-        h.v = 0.0f;
-        inv_d = wf::Vec3{1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
-        node = s.n_nodes > 0 ? 0 : -1;
+        if (shadow_ray) traversal_begin(jn_nodes, ps.ray.o, sh_dir, wf::kRayEps, sh_tmax, &ray, &node, &h);
+        else traversal_begin(jn_nodes, ps.ray.o, ps.ray.d, ps.ray.tmin, ps.ray.tmax, &ray, &node, &h);
     };
 
     for (;;) {
@@ -100,57 +97,13 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
                 const bool waiting = !trav && (pixel >= 0 || !out_of_work);
                 if (__ballot_sync(kFull, waiting) != 0) break;
             }
-            if (!trav) continue;
-            const float4 na = __ldg(&s.nodes[2 * node]);
-            const float4 nb = __ldg(&s.nodes[2 * node + 1]);
-            const int skip = __float_as_int(na.w);
-            wf::Ray r;
-            r.o = ps.ray.o;
-            r.d = rd;
-            r.tmin = r_tmin;
-            r.tmax = h.t;  // the best hit so far bounds the ray (r.tmax = t on every hit)
-            if (!wf::hit_box(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, r.o, inv_d, r.tmin, r.tmax)) {
-                node = skip;
-            } else {
-                const int leaf = __float_as_int(nb.w);
-                if (leaf < 0) {
-                    node = node + 1;
-                } else {
-                    node = skip;
-                    const int count = leaf & kLeafCountMask;
-                    const float4* rec = s.prims + 3 * (leaf >> kLeafCountBits);
-                    for (int i = 0; i < count; ++i, rec += 3) {
-                        const float4 q0 = __ldg(rec);
-                        const float4 q1 = __ldg(rec + 1);
-                        const int p = __float_as_int(q0.w);
-                        float t, u = 0.0f, v = 0.0f;
-                        bool hit;
-                        if (p < s.n_spheres) {
-                            hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
-                        } else {
-                            const float4 q2 = __ldg(rec + 2);
-                            hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
-                                                        wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
-                        }
-                        if (hit) {
-                            r.tmax = t;
-                            h.t = t;
-                            h.prim = p;
-                            h.u = u;
-                            h.v = v;
-                            if (shadow_ray) {  // any-hit: the first hit ends the query
-                                node = -1;
-                                break;
-                            }
-                        }
-                    }
-                }
-            }
-            if (node >= s.n_nodes) node = -1;
+            if (trav) traversal_step(jnodes, jprims, jn_nodes, jn_spheres, ray, shadow_ray, node, h);
         }
 
         // ================= shading: lanes whose ray has finished =================
         if (node < 0 && pixel >= 0) {
+            const JobDesc& J = job_at<MULTI>(a, job);
+            const DevScene& s = J.s;
             bool path_done = false;
             if (shadow_ray) {
                 ++n_shadow;
@@ -165,7 +118,7 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
                     path_done = true;
                 } else {
                     wf::Surface f;
-                    const int mat = wf::classify(s, ps, h, a.max_depth, &f);
+                    const int mat = wf::classify(s, ps, h, J.max_depth, &f);
                     if (mat < 0) {
                         path_done = true;
                     } else if (mat == wf::kLambert) {
@@ -190,8 +143,8 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
                 }
             }
             if (path_done) {
-                if (split) {
-                    float* slot = a.lbuf + 3 * ((size_t)pixel * a.sample_count + (sample - a.first_sample));
+                if (J.chunks > 1) {
+                    float* slot = J.lbuf + 3 * ((size_t)pixel * J.sample_count + (sample - J.first_sample));
                     slot[0] = ps.L.x;
                     slot[1] = ps.L.y;
                     slot[2] = ps.L.z;
@@ -205,14 +158,14 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
                 }
                 ++sample;
                 if (sample < s_end) {
-                    ps = wf::init_path(s, px, py, (uint32_t)sample, a.seed);
+                    ps = wf::init_path(s, px, py, (uint32_t)sample, J.seed);
                 } else {
-                    if (!split) {
-                        a.film.rgb[3 * pixel] = acc_r;
-                        a.film.rgb[3 * pixel + 1] = acc_g;
-                        a.film.rgb[3 * pixel + 2] = acc_b;
-                        a.film.lum[pixel] = acc_l;
-                        a.film.lum2[pixel] = acc_l2;
+                    if (J.chunks == 1) {
+                        J.film.rgb[3 * pixel] = acc_r;
+                        J.film.rgb[3 * pixel + 1] = acc_g;
+                        J.film.rgb[3 * pixel + 2] = acc_b;
+                        J.film.lum[pixel] = acc_l;
+                        J.film.lum2[pixel] = acc_l2;
                     }
                     pixel = -1;
                 }
@@ -231,21 +184,38 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
             if (need) {
                 const unsigned u = base + __popc(need_mask & ((1u << lane) - 1u));
                 if (u < total_units) {
-                    // unit u: pixel u mod P, chunk u div P (neighbouring lanes, neighbouring pixels)
-                    pixel = (int)(u % (unsigned)a.pixels);
-                    const int c = (int)(u / (unsigned)a.pixels);
+                    if (MULTI) {  // last job whose first unit is <= u
+                        int lo = 0, hi = n_jobs - 1;
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (a.jobs[mid].unit_begin <= u) lo = mid;
+                            else hi = mid - 1;
+                        }
+                        job = lo;
+                    }
+                    const JobDesc& J = job_at<MULTI>(a, job);
+                    const DevScene& s = J.s;
+                    jnodes = s.nodes;
+                    jprims = s.prims;
+                    jn_nodes = s.n_nodes;
+                    jn_spheres = s.n_spheres;
+                    // unit -> pixel (u mod P) and chunk (u div P): neighbouring lanes, neighbouring pixels
+                    const unsigned local = u - J.unit_begin;
+                    const int pixels = J.film.pixels;
+                    pixel = (int)(local % (unsigned)pixels);
+                    const int c = (int)(local / (unsigned)pixels);
                     px = pixel % s.width;
                     py = pixel / s.width;
-                    sample = a.first_sample + c * a.chunk;
-                    s_end = min(sample + a.chunk, a.first_sample + a.sample_count);
-                    if (!split) {
-                        acc_r = a.film.rgb[3 * pixel];
-                        acc_g = a.film.rgb[3 * pixel + 1];
-                        acc_b = a.film.rgb[3 * pixel + 2];
-                        acc_l = a.film.lum[pixel];
-                        acc_l2 = a.film.lum2[pixel];
+                    sample = J.first_sample + c * J.chunk;
+                    s_end = min(sample + J.chunk, J.first_sample + J.sample_count);
+                    if (J.chunks == 1) {
+                        acc_r = J.film.rgb[3 * pixel];
+                        acc_g = J.film.rgb[3 * pixel + 1];
+                        acc_b = J.film.rgb[3 * pixel + 2];
+                        acc_l = J.film.lum[pixel];
+                        acc_l2 = J.film.lum2[pixel];
                     }
-                    ps = wf::init_path(s, px, py, (uint32_t)sample, a.seed);
+                    ps = wf::init_path(s, px, py, (uint32_t)sample, J.seed);
                     shadow_ray = false;
                     start_ray();
                 } else {
@@ -271,10 +241,7 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
     }
 }
 
-// Split mode: film_add of every (pixel, sample) slot in ascending sample order.
-__global__ void film_commit(DevFilm film, const float* __restrict__ lbuf, int pixels, int count) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= pixels) return;
+__device__ __forceinline__ void commit_pixel(const DevFilm& film, const float* __restrict__ lbuf, int p, int count) {
     float r = film.rgb[3 * p], g = film.rgb[3 * p + 1], b = film.rgb[3 * p + 2];
     float l1 = film.lum[p], l2 = film.lum2[p];
     const float* slot = lbuf + 3 * (size_t)p * count;
@@ -294,27 +261,54 @@ __global__ void film_commit(DevFilm film, const float* __restrict__ lbuf, int pi
     film.lum2[p] = l2;
 }
 
-template <int BLOCK>
-int resident_lanes(int blocks_per_sm) {
+// Split mode: film_add of every (pixel, sample) slot in ascending sample order.
+__global__ void film_commit(DevFilm film, const float* __restrict__ lbuf, int pixels, int count) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < pixels) commit_pixel(film, lbuf, p, count);
+}
+
+// Batch form: blockIdx.y is the job; jobs in direct mode have nothing to commit.
+__global__ void film_commit_jobs(const JobDesc* jobs, const BatchHeader* hdr) {
+    const int j = blockIdx.y;
+    if (j >= (int)hdr->n_jobs) return;
+    const JobDesc& J = jobs[j];
+    if (J.chunks <= 1) return;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < J.film.pixels; p += gridDim.x * blockDim.x)
+        commit_pixel(J.film, J.lbuf, p, J.sample_count);
+}
+
+template <int BLOCK, bool MULTI>
+int resident_ctas(int blocks_per_sm) {
     int dev = 0, sms = 0, occ = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_persistent<BLOCK>, BLOCK, 0),
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_persistent<BLOCK, MULTI>, BLOCK, 0),
                "occupancy");
     if (blocks_per_sm > 0 && blocks_per_sm < occ) occ = blocks_per_sm;
     if (occ < 1) occ = 1;
-    return sms * occ;  // resident CTAs
+    return sms * occ;
 }
 
-template <int BLOCK>
-void launch_block(const MkArgs& args, int blocks_per_sm, cudaStream_t stream) {
-    long long grid = resident_lanes<BLOCK>(blocks_per_sm);
-    const long long units = (long long)args.pixels * args.chunks;
-    const long long needed = (units + BLOCK - 1) / BLOCK;
-    if (grid > needed) grid = needed;
+template <int BLOCK, bool MULTI>
+void launch_block(const MkArgs& args, long long units, int blocks_per_sm, cudaStream_t stream) {
+    long long grid = resident_ctas<BLOCK, MULTI>(blocks_per_sm);
+    if (units > 0) {
+        const long long needed = (units + BLOCK - 1) / BLOCK;
+        if (grid > needed) grid = needed;
+    }
     if (grid < 1) grid = 1;
-    megakernel_persistent<BLOCK><<<(unsigned)grid, BLOCK, 0, stream>>>(args);
+    megakernel_persistent<BLOCK, MULTI><<<(unsigned)grid, BLOCK, 0, stream>>>(args);
     cuda_check(cudaGetLastError(), "megakernel launch");
+}
+
+template <bool MULTI>
+void launch_any(const MkArgs& args, long long units, const MegakernelConfig& cfg, cudaStream_t stream) {
+    switch (cfg.block) {
+        case 64: launch_block<64, MULTI>(args, units, cfg.blocks_per_sm, stream); break;
+        case 256: launch_block<256, MULTI>(args, units, cfg.blocks_per_sm, stream); break;
+        case 128: launch_block<128, MULTI>(args, units, cfg.blocks_per_sm, stream); break;
+        default: throw Error(WFB_ERR_INVALID_ARGUMENT, "megakernel block size must be 64, 128 or 256");
+    }
 }
 
 }  // namespace
@@ -327,9 +321,9 @@ void launch_film_commit(const DevFilm& film, const float* lbuf, int count, cudaS
 
 int megakernel_resident_threads(const MegakernelConfig& cfg) {
     switch (cfg.block) {
-        case 64: return 64 * resident_lanes<64>(cfg.blocks_per_sm);
-        case 256: return 256 * resident_lanes<256>(cfg.blocks_per_sm);
-        default: return 128 * resident_lanes<128>(cfg.blocks_per_sm);
+        case 64: return 64 * resident_ctas<64, false>(cfg.blocks_per_sm);
+        case 256: return 256 * resident_ctas<256, false>(cfg.blocks_per_sm);
+        default: return 128 * resident_ctas<128, false>(cfg.blocks_per_sm);
     }
 }
 
@@ -343,38 +337,59 @@ int megakernel_split_chunks(int pixels, int sample_count, const MegakernelConfig
     return (int)k;
 }
 
+JobDesc make_job(const DevScene& s, const DevFilm& film, float* lbuf, int first_sample, int sample_count, int chunks,
+                 uint32_t seed, int max_depth) {
+    JobDesc j{};
+    j.s = s;
+    j.film = film;
+    j.lbuf = lbuf;
+    j.first_sample = first_sample;
+    j.sample_count = sample_count;
+    j.chunks = chunks < 1 ? 1 : chunks;
+    j.chunk = sample_count > 0 ? (sample_count + j.chunks - 1) / j.chunks : 0;
+    j.chunks = j.chunk > 0 ? (sample_count + j.chunk - 1) / j.chunk : 1;  // no empty trailing chunk
+    j.seed = seed;
+    j.max_depth = max_depth;
+    j.unit_begin = 0;
+    j.units = sample_count > 0 ? (unsigned)film.pixels * (unsigned)j.chunks : 0u;
+    return j;
+}
+
 void launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters, unsigned int* work_counter,
                        float* lbuf, const PassParams& p, const MegakernelConfig& cfg, int chunks,
                        cudaStream_t stream) {
     if (p.sample_count <= 0 || film.pixels <= 0) return;
     if (chunks > 1 && lbuf == nullptr) throw Error(WFB_ERR_INTERNAL, "split megakernel needs a sample buffer");
-    MkArgs args;
-    args.s = s;
-    args.film = film;
+    MkArgs args{};
+    args.job0 = make_job(s, film, lbuf, p.first_sample, p.sample_count, chunks, p.seed, p.max_depth);
+    args.jobs = nullptr;
+    args.hdr = nullptr;
     args.counters = counters;
     args.work = work_counter;
-    args.lbuf = lbuf;
-    args.pixels = film.pixels;
-    args.first_sample = p.first_sample;
-    args.sample_count = p.sample_count;
-    args.chunks = chunks < 1 ? 1 : chunks;
-    args.chunk = (p.sample_count + args.chunks - 1) / args.chunks;
-    args.chunks = (p.sample_count + args.chunk - 1) / args.chunk;  // no empty trailing chunk
-    args.seed = p.seed;
-    args.max_depth = p.max_depth;
     args.count_rays = p.count_rays ? 1 : 0;
     args.min_active = cfg.min_active;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
-    switch (cfg.block) {
-        case 64: launch_block<64>(args, cfg.blocks_per_sm, stream); break;
-        case 256: launch_block<256>(args, cfg.blocks_per_sm, stream); break;
-        case 128: launch_block<128>(args, cfg.blocks_per_sm, stream); break;
-        default: throw Error(WFB_ERR_INVALID_ARGUMENT, "megakernel block size must be 64, 128 or 256");
-    }
-    if (args.chunks > 1) {
-        film_commit<<<(film.pixels + 255) / 256, 256, 0, stream>>>(film, lbuf, film.pixels, p.sample_count);
-        cuda_check(cudaGetLastError(), "film commit launch");
-    }
+    launch_any<false>(args, args.job0.units, cfg, stream);
+    if (args.job0.chunks > 1) launch_film_commit(film, lbuf, p.sample_count, stream);
+}
+
+void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, int max_jobs, DevCounters* counters,
+                             unsigned int* work_counter, bool count_rays, const MegakernelConfig& cfg,
+                             cudaStream_t stream) {
+    MkArgs args{};
+    args.jobs = d_jobs;
+    args.hdr = d_hdr;
+    args.counters = counters;
+    args.work = work_counter;
+    args.count_rays = count_rays ? 1 : 0;
+    args.min_active = cfg.min_active;
+    cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
+    launch_any<true>(args, 0, cfg, stream);  // full persistent grid: the unit count lives on the device
+    int dev = 0, sms = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    film_commit_jobs<<<dim3((unsigned)sms, (unsigned)std::max(1, max_jobs)), 256, 0, stream>>>(d_jobs, d_hdr);
+    cuda_check(cudaGetLastError(), "film commit launch");
 }
 
 }  // namespace wfb

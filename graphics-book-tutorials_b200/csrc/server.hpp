@@ -1,0 +1,85 @@
+// Render server: continuous batching of render jobs on one GPU (server.cpp).
+#pragma once
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+#include "batch.hpp"
+
+namespace wfb {
+
+struct ServerConfig {
+    uint64_t budget_bytes = 40ull << 30;  // device bytes of admitted jobs (films + sample buffers)
+    int max_jobs = 256;                   // jobs per launch
+    double launch_target_ms = 20.0;       // slice size aims at launches of about this length
+    int fixed_slice = 0;                  // > 0: samples per job per launch (0: adaptive)
+    bool one_job_per_launch = false;      // plain mode: FIFO, whole job, one launch per job
+    bool use_graph = true;
+    MegakernelConfig cfg;
+};
+
+enum JobState : int { kQueued = 0, kActive = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
+
+struct ServerStats {
+    uint64_t submitted = 0, completed = 0, cancelled = 0, failed = 0, launches = 0;
+    uint64_t samples_done = 0;
+    double busy_ms = 0.0;  // device time of all launches
+    double wall_s = 0.0;   // since the first submission
+    double p50_ms = 0.0, p95_ms = 0.0, p99_ms = 0.0, mean_ms = 0.0, max_ms = 0.0;
+    uint64_t bytes_in_use = 0, peak_bytes = 0;
+    int queued = 0, active = 0;
+};
+
+class Server {
+public:
+    explicit Server(const ServerConfig& cfg);
+    ~Server();
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+
+    uint64_t submit(const JobSpec& job);  // thread-safe; the arrival time is now
+    int state(uint64_t ticket);
+    // Waits for completion; false on timeout (timeout_ms < 0: forever).
+    bool wait(uint64_t ticket, int timeout_ms);
+    // Copies the finished film (GPU-arm download convention) and releases the job.
+    void result(uint64_t ticket, float* rgb, float* lum_var, double* latency_ms);
+    bool cancel(uint64_t ticket);
+    ServerStats stats();
+    void reset_stats();
+    void shutdown();
+
+private:
+    struct Job;
+    void worker();
+    uint64_t job_bytes(const Job& j) const;
+    bool admit_locked();
+    int choose_slice(const std::vector<Job*>& act);
+
+    ServerConfig cfg_;
+    std::unique_ptr<BatchLauncher> launcher_;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    std::mutex mu_;
+    std::condition_variable cv_work_, cv_done_;
+    std::map<uint64_t, std::unique_ptr<Job>> jobs_;
+    std::deque<uint64_t> queue_;
+    std::vector<uint64_t> active_;
+    uint64_t next_ticket_ = 1;
+    bool stop_ = false;
+    std::thread thread_;
+    uint64_t bytes_in_use_ = 0, peak_bytes_ = 0;
+    double msps_estimate_ = 200.0;  // Msamples/s, refined after every launch
+    std::vector<double> latencies_ms_;
+    ServerStats st_;
+    double t_first_ = -1.0;
+    int device_ = 0;
+};
+
+double now_seconds();
+
+}  // namespace wfb

@@ -155,6 +155,73 @@ int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */
 int wfb_renderer_destroy(wfb_renderer_t r);
 
+/* ---- batched rendering (no reference counterpart: one scene/camera/job per GpuRenderer) -------
+ * Many jobs of uneven size rendered in ONE persistent launch, replayed through a CUDA graph
+ * captured once per launch shape. Every job's film is bit-identical to the same job rendered
+ * alone by wfb_renderer_render. */
+typedef struct wfb_batch* wfb_batch_t;
+typedef struct {
+    float cam_position[3], cam_look_at[3], cam_up[3];
+    float cam_vfov_deg;
+    int width, height;
+    int spp;
+    uint32_t seed;
+    int max_depth;
+} wfb_job_desc;
+/* use_graph != 0: replay one captured graph per launch shape. block/min_active <= 0: defaults. */
+int wfb_batch_create(int max_jobs, int use_graph, int block, int min_active, wfb_batch_t* out);
+int wfb_batch_add(wfb_batch_t b, wfb_scene_t scene, const wfb_job_desc* job, int* job_id);
+int wfb_batch_clear(wfb_batch_t b);
+/* Zeroes all films, renders every job in one launch, waits; stats may be NULL. */
+int wfb_batch_run(wfb_batch_t b, int count_rays, wfb_render_stats* stats);
+/* GPU-arm download convention of job `job_id` (rgb 3*w*h, lum_var w*h, either may be NULL). */
+int wfb_batch_download(wfb_batch_t b, int job_id, float* rgb, float* lum_var);
+int wfb_batch_download_sums(wfb_batch_t b, int job_id, float* rgb_sum, float* lum_sum, float* lum2_sum);
+int wfb_batch_destroy(wfb_batch_t b);
+
+/* ---- render server (no reference counterpart) -------------------------------------------------
+ * Continuous batching: a worker thread admits queued jobs while their device bytes fit the budget,
+ * and every launch advances all admitted jobs by a slice of samples sized to take about
+ * launch_target_ms, so requests arriving during a launch join the next one. Latency is measured
+ * from wfb_server_submit to the film being ready on the host. one_job_per_launch = 1 gives the
+ * sequential baseline (FIFO, one launch per whole job). */
+typedef struct wfb_server* wfb_server_t;
+typedef struct {
+    uint64_t budget_bytes;   /* 0: 40 GiB */
+    int max_jobs;            /* per launch; 0: 256 */
+    double launch_target_ms; /* 0: 20 */
+    int fixed_slice;         /* > 0: samples per job per launch */
+    int one_job_per_launch;
+    int use_graph;
+    int block, min_active;   /* <= 0: defaults */
+} wfb_server_config;
+typedef struct {
+    uint64_t submitted, completed, cancelled, failed, launches, samples_done;
+    double busy_ms, wall_s;
+    double p50_ms, p95_ms, p99_ms, mean_ms, max_ms;
+    uint64_t bytes_in_use, peak_bytes;
+    int queued, active;
+} wfb_server_stats;
+#define WFB_JOB_QUEUED 0
+#define WFB_JOB_ACTIVE 1
+#define WFB_JOB_DONE 2
+#define WFB_JOB_CANCELLED 3
+#define WFB_JOB_FAILED 4
+int wfb_server_create(const wfb_server_config* cfg, wfb_server_t* out);
+/* Thread-safe. The scene must stay alive until the job is finished. */
+int wfb_server_submit(wfb_server_t s, wfb_scene_t scene, const wfb_job_desc* job, uint64_t* ticket);
+int wfb_server_poll(wfb_server_t s, uint64_t ticket, int* state);
+/* WFB_ERR_TIMEOUT when the job is not finished after timeout_ms (< 0: wait forever). */
+int wfb_server_wait(wfb_server_t s, uint64_t ticket, int timeout_ms);
+/* Film of a finished job (GPU-arm convention) and its latency; releases the job. */
+int wfb_server_result(wfb_server_t s, uint64_t ticket, float* rgb, float* lum_var, double* latency_ms);
+/* Drops a queued or running job (running jobs leave at the next launch boundary). */
+int wfb_server_cancel(wfb_server_t s, uint64_t ticket);
+int wfb_server_stats_get(wfb_server_t s, wfb_server_stats* out);
+/* Clears latency samples and counters (keeps jobs in flight). */
+int wfb_server_reset_stats(wfb_server_t s);
+int wfb_server_destroy(wfb_server_t s);
+
 /* ---- queue primitives (WVM/src/gpu/queues.cuh:30-55) ------------------------------------------
  * Device pointers in, stream-ordered, no host synchronisation. Status 1 (WFB_ERR_INVALID_ARGUMENT,
  * the value of cudaErrorInvalidValue the reference returns) for n > capacity, with nothing enqueued.
