@@ -192,6 +192,86 @@ def cpu_baseline(wfb, seconds_target=12.0):
             "kind": kind, "sample": f"{WIDTH}x{HEIGHT} at {spp2} spp (of {SPP}), seed {SEED}, depth {DEPTH}"}
 
 
+def mix_scenes(wfb):
+    return {name: wfb.Scene.generate(name, 64, 64, SEED, 16) for name in wfb.MIX_SCENES}
+
+
+def bench_batch(wfb, scenes, n_jobs=64, repeats=2):
+    """Config 4: the 64-job mix in one persistent launch (graph replay) vs the same jobs rendered
+    one job per launch through GpuRenderer, on the same GPU. Device time for both."""
+    mix = wfb.job_mix(n_jobs, SEED)
+    jobs = [(scenes[m["scene"]], wfb.mix_job_desc(m, scenes[m["scene"]])) for m in mix]
+    samples = sum(j.width * j.height * j.spp for _, j in jobs)
+    b = wfb.Batch(max_jobs=n_jobs, use_graph=True)
+    for s, j in jobs:
+        b.add(s, j)
+    b.run()  # warm-up + graph capture
+    batch_ms = min(b.run().render_ms for _ in range(repeats))
+    seq_ms = 0.0
+    renderers = {}
+    for s, j in jobs:
+        key = id(s)
+        if key not in renderers:
+            renderers[key] = wfb.GpuRenderer(s, wfb.MEGAKERNEL)
+        r = renderers[key]
+        r.set_camera(j.cam_position, j.cam_look_at, j.cam_up, j.cam_vfov_deg, j.width, j.height)
+        st = wfb.RenderStats()
+        r.render(wfb.RenderParams(spp=j.spp, seed=j.seed, max_depth=j.max_depth), st)
+        seq_ms += st.render_ms
+    b.close()
+    return {"jobs": n_jobs, "samples": samples, "batched_ms": round(batch_ms, 2),
+            "batched_msamples_s": round(samples / batch_ms / 1e3, 2),
+            "one_job_per_launch_ms": round(seq_ms, 2),
+            "one_job_per_launch_msamples_s": round(samples / seq_ms / 1e3, 2),
+            "speedup": round(seq_ms / batch_ms, 3), "graph": True}
+
+
+def bench_serve(wfb, scenes, lam, duration, drain=30.0, plain=False, seed=SEED, target_ms=20.0):
+    """Config 5: open-loop Poisson arrivals at `lam` jobs/s for `duration` s from the config-4 mix;
+    latency = submit -> film on the host. Jobs still running `drain` s after the last arrival are
+    reported as incomplete (and their latency is not in the percentiles)."""
+    import threading
+    mix = wfb.job_mix(64, SEED)
+    descs = [(scenes[m["scene"]], wfb.mix_job_desc(m, scenes[m["scene"]])) for m in mix]
+    rng = np.random.default_rng(seed + int(lam * 1000))
+    srv = wfb.Server(one_job_per_launch=plain, launch_target_ms=target_ms)
+    # warm-up: one small job (graph capture, module load)
+    w = srv.submit(*descs[min(range(64), key=lambda i: descs[i][1].width * descs[i][1].height * descs[i][1].spp)])
+    srv.wait(w, 60000)
+    srv.result(w)
+    srv.reset_stats()
+    tickets = []
+    done_flag = threading.Event()
+    t0 = time.perf_counter()
+    t_next = t0
+    while True:
+        t_next += rng.exponential(1.0 / lam)
+        if t_next - t0 > duration:
+            break
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        s, j = descs[int(rng.integers(64))]
+        tickets.append(srv.submit(s, j))
+    submitted = len(tickets)
+    deadline = time.perf_counter() + drain
+    completed = 0
+    for t in tickets:
+        left = int(max(0.0, deadline - time.perf_counter()) * 1000)
+        if srv.wait(t, left):
+            srv.result(t)
+            completed += 1
+    done_flag.set()
+    st = srv.stats()
+    srv.close()
+    return {"lambda": lam, "duration_s": duration, "submitted": submitted, "completed": completed,
+            "incomplete": submitted - completed, "p50_ms": round(st["p50_ms"], 2), "p95_ms": round(st["p95_ms"], 2),
+            "p99_ms": round(st["p99_ms"], 2), "mean_ms": round(st["mean_ms"], 2),
+            "msamples_s": round(st["samples_done"] / max(st["wall_s"], 1e-9) / 1e6, 2),
+            "busy_frac": round(st["busy_ms"] / 1e3 / max(st["wall_s"], 1e-9), 3), "launches": st["launches"],
+            "mode": "one-job-per-launch" if plain else "continuous-batching"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -204,6 +284,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--size", default=None, help="WxH override (profiling cases only; not a bench line)")
     ap.add_argument("--spp", type=int, default=None, help="spp override (profiling cases only)")
+    ap.add_argument("--mode", default="render", choices=["render", "batch", "serve"],
+                    help="render: config 2 headline line; batch: config 4; serve: config 5 lambda sweep")
+    ap.add_argument("--lambdas", default="5,10,20,50,100,200")
+    ap.add_argument("--duration", type=float, default=60.0)
+    ap.add_argument("--no-batch-serve", action="store_true", help="skip the batched/served summary in render mode")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global WIDTH, HEIGHT, SPP, WORKLOAD
@@ -220,6 +305,20 @@ def main():
     import torch
     torch.cuda.set_device(local)
     wfb = load_engine()
+    if args.mode in ("batch", "serve"):
+        scenes = mix_scenes(wfb)
+        if args.mode == "batch":
+            out = {"mode": "batch", "workload": "config-4 job mix (64 jobs, seed 1234)", **bench_batch(wfb, scenes)}
+            out["device"] = wfb.device_name()
+            print(json.dumps(out), flush=True)
+        else:
+            for lam in [float(x) for x in args.lambdas.split(",")]:
+                for plain in (False, True):
+                    r = bench_serve(wfb, scenes, lam, args.duration, plain=plain)
+                    print(json.dumps({"mode": "serve", **r}), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     mode = wfb.MEGAKERNEL if args.arm == "megakernel" else wfb.WAVEFRONT
     scene = wfb.Scene.generate(SCENE, WIDTH, HEIGHT, SEED, 16)
     host_arrays = scene.export()
@@ -311,6 +410,10 @@ def main():
         "clocks": clk,
         "device": wfb.device_name(),
     }
+    if rank == 0 and not args.no_batch_serve:
+        scenes = mix_scenes(wfb)
+        line["batched"] = bench_batch(wfb, scenes, repeats=1)
+        line["served"] = bench_serve(wfb, scenes, lam=10.0, duration=10.0, drain=20.0)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wfb)
     if rank == 0:

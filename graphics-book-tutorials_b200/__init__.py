@@ -92,7 +92,8 @@ class _CRenderStats(ctypes.Structure):
                 ("extension_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
                 ("queue_high_water", ctypes.c_int64 * 5), ("queue_overflows", ctypes.c_int64),
                 ("invalid_hits", ctypes.c_int64), ("peak_vram_bytes", ctypes.c_uint64),
-                ("stage_ms", ctypes.c_double * 8)]
+                ("stage_ms", ctypes.c_double * 8), ("node_visits", ctypes.c_uint64),
+                ("prim_tests", ctypes.c_uint64)]
 
 
 STAGE_NAMES = ("extend", "classify", "shade_lambert", "shade_metal", "shade_dielectric", "shadow",
@@ -128,12 +129,15 @@ class RenderStats:
     invalid_hits: int = 0
     peak_vram_bytes: int = 0
     stages: dict = field(default_factory=dict)
+    node_visits: int = 0  # megakernel with count_rays: BVH nodes visited
+    prim_tests: int = 0   # megakernel with count_rays: primitive tests
 
     @classmethod
     def _from_c(cls, c: _CRenderStats) -> "RenderStats":
         return cls(c.render_ms, c.total_ms, int(c.extension_rays), int(c.shadow_rays),
                    [int(v) for v in c.queue_high_water], int(c.queue_overflows), int(c.invalid_hits),
-                   int(c.peak_vram_bytes), {n: float(c.stage_ms[i]) for i, n in enumerate(STAGE_NAMES)})
+                   int(c.peak_vram_bytes), {n: float(c.stage_ms[i]) for i, n in enumerate(STAGE_NAMES)},
+                   int(c.node_visits), int(c.prim_tests))
 
 
 @dataclass
@@ -171,6 +175,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_scene_info_get": (i32, [vp, ctypes.POINTER(SceneInfo)]),
         "wfb_scene_export": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "wfb_scene_hash": (u64, [vp]),
+        "wfb_scene_rebuild_bvh": (i32, [vp, i32, i32, ctypes.c_float]),
         "wfb_scene_validate_bvh": (i32, [vp, ctypes.c_char_p, i32]),
         "wfb_scene_destroy": (i32, [vp]),
         "wfb_scene_device_bytes": (u64, [vp]),
@@ -184,7 +189,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_renderer_download_sums": (i32, [vp, vp, vp, vp]),
         "wfb_renderer_render": (i32, [vp, ctypes.POINTER(_CRenderParams), ctypes.POINTER(_CRenderStats), vp, vp]),
         "wfb_renderer_device_bytes": (u64, [vp]),
-        "wfb_renderer_configure": (i32, [vp, i32, i32, i32, i32, i32]),
+        "wfb_renderer_configure": (i32, [vp, i32, i32, i32, i32, i32, i32]),
         "wfb_renderer_width": (i32, [vp]),
         "wfb_renderer_height": (i32, [vp]),
         "wfb_renderer_destroy": (i32, [vp]),
@@ -277,6 +282,10 @@ class Scene:
 
     def hash(self) -> int:
         return int(load_library().wfb_scene_hash(self._h))
+
+    def rebuild_bvh(self, bins: int = 16, max_leaf: int = 4, traversal_cost: float = 1.0) -> None:
+        """Rebuilds the BVH with SAH knobs (before the first upload); see wfb_scene_rebuild_bvh."""
+        _check(load_library().wfb_scene_rebuild_bvh(self._h, int(bins), int(max_leaf), float(traversal_cost)))
 
     def validate_bvh(self) -> str:
         buf = ctypes.create_string_buffer(256)
@@ -371,11 +380,11 @@ class GpuRenderer:
     def device_bytes(self) -> int:
         return int(load_library().wfb_renderer_device_bytes(self._h))
 
-    def configure(self, block: int = 0, blocks_per_sm: int = 0, min_active: int = 0, split_chunks: int = 0,
-                  paths_in_flight: int = 0) -> None:
-        """Launch knobs (values <= 0 keep the current setting); see wfb_renderer_configure."""
+    def configure(self, block: int = -1, blocks_per_sm: int = -1, min_active: int = -1, split_chunks: int = -1,
+                  paths_in_flight: int = -1, occupancy: int = -1) -> None:
+        """Launch knobs (-1 keeps the current setting); see wfb_renderer_configure."""
         _check(load_library().wfb_renderer_configure(self._h, block, blocks_per_sm, min_active, split_chunks,
-                                                      paths_in_flight))
+                                                      paths_in_flight, occupancy))
 
     def close(self) -> None:
         if self._h is not None and self._h.value:

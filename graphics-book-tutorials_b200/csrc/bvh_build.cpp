@@ -16,7 +16,9 @@
 //                  so this mode reproduces the reference's tree node for node (pinned by a test).
 //   sah_bins != 8  (default 16 for the benchmark scenes): all three axes are binned and the
 //                  cheapest split wins; a node with <= 4 primitives becomes a leaf unless a split
-//                  is cheaper under the surface-area heuristic (traversal cost 1, intersection 1).
+//                  is cheaper under the surface-area heuristic (traversal cost 0.5, intersection 1:
+//                  measured fastest for the stackless traversal, where primitive tests cost more
+//                  than box tests).
 #include <algorithm>
 #include <stdexcept>
 #include <vector>
@@ -82,7 +84,8 @@ struct Work {
 
 class Builder {
 public:
-    Builder(const Scene& scene, int bins) : info_(prim_infos(scene)), bins_(bins) {
+    Builder(const Scene& scene, int bins, int max_leaf, float traversal_cost)
+        : info_(prim_infos(scene)), bins_(bins), max_leaf_(max_leaf), ct_(traversal_cost) {
         ids_.resize(info_.size());
         for (int i = 0; i < (int)ids_.size(); ++i) ids_[i] = i;
     }
@@ -151,7 +154,7 @@ private:
         if (n <= 1) return true;
         const Vec3 ext = cbounds.hi - cbounds.lo;
         if (ext.x < 1e-6f && ext.y < 1e-6f && ext.z < 1e-6f) {
-            if (n <= 4) return true;
+            if (n <= max_leaf_) return true;
             *mid = begin + n / 2;
             return false;
         }
@@ -207,10 +210,10 @@ private:
                 }
             }
         }
-        if (!compat && n <= 4) {
+        if (!compat && n <= max_leaf_) {
             // SAH termination: a leaf costs n intersections; a split costs one more node visit
-            // plus the area-weighted intersections of its children.
-            if (best_axis < 0 || (float)n <= 1.0f + best_cost) return true;
+            // (traversal_cost) plus the area-weighted intersections of its children.
+            if (best_axis < 0 || (float)n <= ct_ + best_cost) return true;
         }
         int m = begin;
         if (best_axis >= 0) {
@@ -231,17 +234,23 @@ private:
     std::vector<PrimInfo> info_;
     std::vector<int> ids_;
     int bins_;
+    int max_leaf_;
+    float ct_;
 };
 
 }  // namespace
 
-void build_bvh_bins(Scene& scene, int sah_bins) {
+void build_bvh_options(Scene& scene, int sah_bins, int max_leaf, float traversal_cost) {
     if (scene.spheres.empty() && scene.triangles.empty())
         throw std::runtime_error("Cannot build BVH: no primitives");
     if (sah_bins < 2 || sah_bins > 256) throw std::runtime_error("SAH bin count must be in [2, 256]");
-    Builder b(scene, sah_bins);
+    if (max_leaf < 1 || max_leaf > 15) throw std::runtime_error("max_leaf must be in [1, 15]");
+    if (!(traversal_cost >= 0.0f)) throw std::runtime_error("traversal cost must be >= 0");
+    Builder b(scene, sah_bins, sah_bins == 8 ? 4 : max_leaf, traversal_cost);
     b.run(&scene.nodes, &scene.prim_order);
 }
+
+void build_bvh_bins(Scene& scene, int sah_bins) { build_bvh_options(scene, sah_bins, 4, 0.5f); }
 
 void build_bvh(Scene& scene) { build_bvh_bins(scene, 8); }
 

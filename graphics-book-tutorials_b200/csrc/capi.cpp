@@ -109,6 +109,8 @@ void to_c_stats(const wf::RenderStats& s, wfb_render_stats* out) {
     const double st[8] = {s.stages.extend, s.stages.classify, s.stages.shade_lambert, s.stages.shade_metal,
                           s.stages.shade_dielectric, s.stages.shadow, s.stages.compact, s.stages.other};
     for (int i = 0; i < 8; ++i) out->stage_ms[i] = st[i];
+    out->node_visits = 0;
+    out->prim_tests = 0;
 }
 
 void need(bool ok, const char* msg) {
@@ -227,6 +229,15 @@ int wfb_scene_export(wfb_scene_t s, void* spheres, float* vertices, int* triangl
 
 uint64_t wfb_scene_hash(wfb_scene_t s) { return s ? wf::scene_hash(s->host) : 0; }
 
+int wfb_scene_rebuild_bvh(wfb_scene_t s, int bins, int max_leaf, float traversal_cost) {
+    return guarded([&] {
+        need(s != nullptr, "null scene");
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->resident) throw wfb::Error(WFB_ERR_INVALID_ARGUMENT, "scene is already uploaded; rebuild before use");
+        wf::build_bvh_options(s->host, bins, max_leaf, traversal_cost);
+    });
+}
+
 int wfb_scene_validate_bvh(wfb_scene_t s, char* msg, int len) {
     return guarded([&] {
         need(s && msg && len > 0, "null argument");
@@ -285,7 +296,11 @@ int wfb_renderer_run_passes(wfb_renderer_t r, int first_sample, int count, const
         need(r && p, "null argument");
         wf::RenderStats st{};
         r->r->run_passes(pass_params(p, first_sample, count), &st);
-        if (stats) to_c_stats(st, stats);
+        if (stats) {
+            to_c_stats(st, stats);
+            stats->node_visits = r->r->last_node_visits();
+            stats->prim_tests = r->r->last_prim_tests();
+        }
     });
 }
 
@@ -319,19 +334,25 @@ int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render
         wf::RenderStats st{};
         r->r->run_passes(pass_params(p, 0, p->spp), &st);
         r->r->download(p->spp, rgb, lum_var);
-        if (stats) to_c_stats(st, stats);
+        if (stats) {
+            to_c_stats(st, stats);
+            stats->node_visits = r->r->last_node_visits();
+            stats->prim_tests = r->r->last_prim_tests();
+        }
     });
 }
 
 uint64_t wfb_renderer_device_bytes(wfb_renderer_t r) { return r ? r->r->device_bytes() : 0; }
 
 int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int min_active, int split_chunks,
-                           int paths_in_flight) {
+                           int paths_in_flight, int occupancy) {
     return guarded([&] {
         need(r != nullptr, "null renderer");
         need(block <= 0 || block == 64 || block == 128 || block == 256, "block must be 64, 128 or 256");
         need(min_active <= 32, "min_active must be in 1..32");
-        r->r->configure(block, blocks_per_sm, min_active, split_chunks, paths_in_flight);
+        need(occupancy < 0 || occupancy == 0 || ((occupancy == 6 || occupancy == 8) && (block <= 0 || block == 128)),
+             "occupancy target must be 0, 6 or 8 (block 128)");
+        r->r->configure(block, blocks_per_sm, min_active, split_chunks, paths_in_flight, occupancy);
     });
 }
 int wfb_renderer_width(wfb_renderer_t r) { return r ? r->r->width() : 0; }

@@ -175,10 +175,37 @@ __device__ __forceinline__ bool intersect_dev(const DevScene& s, wf::Ray r, wf::
     return h->prim >= 0;
 }
 
-// A ray being traversed by the resumable form of the traversal below.
+// Slab test of wf::hit_box without the two early exits: t0 only grows and t1 only shrinks
+// (compare-and-select updates that keep the reference's NaN behaviour), so once t0 > t1 the final
+// t0 <= t1 is false as well -- the result is identical, with fewer branches.
+__device__ __forceinline__ bool hit_box_nobranch(wf::Vec3 lo, wf::Vec3 hi, wf::Vec3 o, wf::Vec3 inv_d, float tmin,
+                                                 float tmax) {
+    float t0 = tmin, t1 = tmax;
+    float tn = (lo.x - o.x) * inv_d.x, tf = (hi.x - o.x) * inv_d.x;
+    float a = tn > tf ? tf : tn, b = tn > tf ? tn : tf;
+    t0 = a > t0 ? a : t0;
+    t1 = b < t1 ? b : t1;
+    tn = (lo.y - o.y) * inv_d.y;
+    tf = (hi.y - o.y) * inv_d.y;
+    a = tn > tf ? tf : tn;
+    b = tn > tf ? tn : tf;
+    t0 = a > t0 ? a : t0;
+    t1 = b < t1 ? b : t1;
+    tn = (lo.z - o.z) * inv_d.z;
+    tf = (hi.z - o.z) * inv_d.z;
+    a = tn > tf ? tf : tn;
+    b = tn > tf ? tn : tf;
+    t0 = a > t0 ? a : t0;
+    t1 = b < t1 ? b : t1;
+    return t0 <= t1;
+}
+
+// Direction of a ray being traversed by the resumable traversal below. Its origin is passed to
+// each step (the path's current ray origin) and its tmin is kRayEps: every ray the estimator
+// creates has tmin = kRayEps (camera_ray, set_next_ray, the shadow ray of shade_lambert,
+// WVM/include/wf/path_core.hpp:67,184,211), so neither is stored per ray.
 struct TravRay {
-    wf::Vec3 o, d, inv_d;
-    float tmin;
+    wf::Vec3 d, inv_d;
 };
 
 // One step of the stackless skip-link traversal, resumable between calls: the whole state is the
@@ -186,17 +213,17 @@ struct TravRay {
 // order, box and primitive arithmetic and the strictly-nearer rule are intersect_dev's, so running
 // steps until node < 0 gives bit-identical hits. `anyhit` ends the query at the first hit.
 __device__ __forceinline__ void traversal_step(const float4* __restrict__ nodes, const float4* __restrict__ prims,
-                                               int n_nodes, int n_spheres, const TravRay& ray, bool anyhit,
-                                               int& node, wf::HitRecord& h) {
+                                               int n_nodes, int n_spheres, const wf::Vec3& o, const TravRay& ray,
+                                               bool anyhit, int& node, wf::HitRecord& h, unsigned& n_prim_tests) {
     const float4 na = __ldg(&nodes[2 * node]);
     const float4 nb = __ldg(&nodes[2 * node + 1]);
     const int skip = __float_as_int(na.w);
     wf::Ray r;
-    r.o = ray.o;
+    r.o = o;
     r.d = ray.d;
-    r.tmin = ray.tmin;
+    r.tmin = wf::kRayEps;
     r.tmax = h.t;
-    if (!wf::hit_box(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, r.o, ray.inv_d, r.tmin, r.tmax)) {
+    if (!hit_box_nobranch(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, r.o, ray.inv_d, r.tmin, r.tmax)) {
         node = skip;
     } else {
         const int leaf = __float_as_int(nb.w);
@@ -212,6 +239,7 @@ __device__ __forceinline__ void traversal_step(const float4* __restrict__ nodes,
                 const int p = __float_as_int(q0.w);
                 float t, u = 0.0f, v = 0.0f;
                 bool hit;
+                ++n_prim_tests;
                 if (p < n_spheres) {
                     hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
                 } else {
@@ -237,11 +265,9 @@ __device__ __forceinline__ void traversal_step(const float4* __restrict__ nodes,
 }
 
 // intersect() prologue (WVM/include/wf/bvh.hpp:92-94): the ray's traversal state before step 0.
-__device__ __forceinline__ void traversal_begin(int n_nodes, wf::Vec3 o, wf::Vec3 d, float tmin, float tmax,
-                                                TravRay* ray, int* node, wf::HitRecord* h) {
-    ray->o = o;
+__device__ __forceinline__ void traversal_begin(int n_nodes, wf::Vec3 d, float tmax, TravRay* ray, int* node,
+                                                wf::HitRecord* h) {
     ray->d = d;
-    ray->tmin = tmin;
     ray->inv_d = wf::Vec3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
     h->t = tmax;
     h->prim = -1;
@@ -276,6 +302,9 @@ struct DevCounters {
     unsigned int overflows;
     unsigned int high_water[5];
     unsigned int error;  // nonzero: a bounded wait gave up (see kErr* codes)
+    unsigned int pad;
+    unsigned long long node_visits;  // traversal steps (box tests), when counting rays
+    unsigned long long prim_tests;   // primitive intersection tests, when counting rays
 };
 
 enum : unsigned int {

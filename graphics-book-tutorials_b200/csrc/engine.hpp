@@ -52,8 +52,9 @@ struct PassParams {
 struct MegakernelConfig {
     int block = 128;        // threads per CTA (64, 128 or 256)
     int blocks_per_sm = 0;  // 0: as many as fit
-    int min_active = 20;    // traverse on while at least this many lanes of a warp traverse
+    int min_active = 24;    // traverse on while at least this many lanes of a warp traverse
     int split_chunks = 0;   // work units per pixel; 0: chosen from pixels vs resident lanes
+    int occupancy = 8;      // block 128 only: 6 or 8 caps registers for that many CTAs per SM (0: none)
 };
 // Resident threads of the persistent megakernel for this configuration.
 int megakernel_resident_threads(const MegakernelConfig& cfg);
@@ -115,6 +116,9 @@ public:
     void set_camera(const wf::Camera& cam, int width, int height);
     void reset();
     void run_passes(const PassParams& p, wf::RenderStats* stats);
+    // Traversal counts of the last run_passes with count_rays (megakernel only).
+    uint64_t last_node_visits() const { return last_node_visits_; }
+    uint64_t last_prim_tests() const { return last_prim_tests_; }
     // Reference download convention (WVM/src/gpu/gpu_renderer.cu:306-341).
     void download(int spp_done, float* rgb, float* lum_var);
     void download_mean(int spp_done, float* rgb);
@@ -126,8 +130,9 @@ public:
     wf::GpuMode mode() const { return mode_; }
     void set_megakernel_config(const MegakernelConfig& c) { mk_cfg_ = c; }
     const MegakernelConfig& megakernel_config() const { return mk_cfg_; }
-    // Values <= 0 keep the current setting.
-    void configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight);
+    // Values < 0 keep the current setting (block and min_active also keep on 0).
+    void configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight,
+                   int occupancy);
 
 private:
     void alloc_film();
@@ -145,6 +150,7 @@ private:
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     MegakernelConfig mk_cfg_{};
     WavefrontConfig wf_cfg_{};
+    uint64_t last_node_visits_ = 0, last_prim_tests_ = 0;
     struct Wavefront;
     std::unique_ptr<Wavefront> wf_;
 };

@@ -30,6 +30,7 @@
 //    contribution are kept.
 //  * Ray counters live in registers and are folded with one atomic per warp at exit.
 #include <algorithm>
+#include <type_traits>
 #include "engine.hpp"
 #include "../../include/wfb200.h"
 
@@ -53,37 +54,44 @@ __device__ __forceinline__ const JobDesc& job_at(const MkArgs& a, int j) {
     return MULTI ? a.jobs[j] : a.job0;
 }
 
-template <int BLOCK, bool MULTI>
-__global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
+// MINB > 1 caps registers so that MINB CTAs fit an SM (__launch_bounds__ minimum blocks).
+// COUNT adds node-visit and primitive-test counters (used by count_rays runs only).
+template <int BLOCK, bool MULTI, int MINB, bool COUNT>
+__global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArgs a) {
     const int lane = threadIdx.x & 31;
     const unsigned total_units = MULTI ? a.hdr->total_units : a.job0.units;
     const int n_jobs = MULTI ? (int)a.hdr->n_jobs : 1;
 
     // ---- per-lane work and path state ----
     int job = 0;
-    int pixel = -1, px = 0, py = 0, sample = 0, s_end = 0;
+    int pixel = -1, sample = 0, s_end = 0;
     bool out_of_work = false;
     wf::PathState ps{};
     float acc_r = 0.f, acc_g = 0.f, acc_b = 0.f, acc_l = 0.f, acc_l2 = 0.f;
     bool shadow_ray = false, alive_after_shadow = false;
     wf::Vec3 sh_dir{0.f, 0.f, 0.f}, sh_contrib{0.f, 0.f, 0.f};
     float sh_tmax = 0.f;
-    // ---- traversal state of the lane's current ray (+ the job's BVH, cached) ----
+    // ---- traversal state of the lane's current ray. Every ray starts at ps.ray.o (the camera,
+    // or p + n * eps for both the next extension ray and the shadow ray) with tmin = kRayEps. ----
     int node = -1;
     TravRay ray;
     wf::HitRecord h;
     h.t = 0.f;
     h.prim = -1;
     h.u = h.v = 0.f;
-    const float4* jnodes = a.job0.s.nodes;
-    const float4* jprims = a.job0.s.prims;
-    int jn_nodes = a.job0.s.n_nodes, jn_spheres = a.job0.s.n_spheres;
-    unsigned long long n_ext = 0, n_shadow = 0;
-    unsigned int n_invalid = 0;
+    // batch launches cache the lane's job BVH; a single job reads it from parameter space
+    const float4* jnodes = nullptr;
+    const float4* jprims = nullptr;
+    int jn_nodes = 0, jn_spheres = 0;
+    unsigned n_ext = 0, n_shadow = 0, n_invalid = 0, n_steps = 0, n_prims = 0;
 
     auto start_ray = [&]() {
-        if (shadow_ray) traversal_begin(jn_nodes, ps.ray.o, sh_dir, wf::kRayEps, sh_tmax, &ray, &node, &h);
-        else traversal_begin(jn_nodes, ps.ray.o, ps.ray.d, ps.ray.tmin, ps.ray.tmax, &ray, &node, &h);
+        const int nn = MULTI ? jn_nodes : a.job0.s.n_nodes;
+        if (shadow_ray) traversal_begin(nn, sh_dir, sh_tmax, &ray, &node, &h);
+        else traversal_begin(nn, ps.ray.d, ps.ray.tmax, &ray, &node, &h);
+    };
+    auto new_path = [&](const DevScene& s, uint32_t seed) {
+        ps = wf::init_path(s, pixel % s.width, pixel / s.width, (uint32_t)sample, seed);
     };
 
     for (;;) {
@@ -97,7 +105,14 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
                 const bool waiting = !trav && (pixel >= 0 || !out_of_work);
                 if (__ballot_sync(kFull, waiting) != 0) break;
             }
-            if (trav) traversal_step(jnodes, jprims, jn_nodes, jn_spheres, ray, shadow_ray, node, h);
+            if (trav) {
+                if (COUNT) ++n_steps;
+                if (MULTI)
+                    traversal_step(jnodes, jprims, jn_nodes, jn_spheres, ps.ray.o, ray, shadow_ray, node, h, n_prims);
+                else
+                    traversal_step(a.job0.s.nodes, a.job0.s.prims, a.job0.s.n_nodes, a.job0.s.n_spheres, ps.ray.o, ray,
+                                   shadow_ray, node, h, n_prims);
+            }
         }
 
         // ================= shading: lanes whose ray has finished =================
@@ -158,7 +173,7 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
                 }
                 ++sample;
                 if (sample < s_end) {
-                    ps = wf::init_path(s, px, py, (uint32_t)sample, J.seed);
+                    new_path(s, J.seed);
                 } else {
                     if (J.chunks == 1) {
                         J.film.rgb[3 * pixel] = acc_r;
@@ -195,17 +210,17 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
                     }
                     const JobDesc& J = job_at<MULTI>(a, job);
                     const DevScene& s = J.s;
-                    jnodes = s.nodes;
-                    jprims = s.prims;
-                    jn_nodes = s.n_nodes;
-                    jn_spheres = s.n_spheres;
+                    if (MULTI) {
+                        jnodes = s.nodes;
+                        jprims = s.prims;
+                        jn_nodes = s.n_nodes;
+                        jn_spheres = s.n_spheres;
+                    }
                     // unit -> pixel (u mod P) and chunk (u div P): neighbouring lanes, neighbouring pixels
                     const unsigned local = u - J.unit_begin;
                     const int pixels = J.film.pixels;
                     pixel = (int)(local % (unsigned)pixels);
                     const int c = (int)(local / (unsigned)pixels);
-                    px = pixel % s.width;
-                    py = pixel / s.width;
                     sample = J.first_sample + c * J.chunk;
                     s_end = min(sample + J.chunk, J.first_sample + J.sample_count);
                     if (J.chunks == 1) {
@@ -215,7 +230,7 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
                         acc_l = J.film.lum[pixel];
                         acc_l2 = J.film.lum2[pixel];
                     }
-                    ps = wf::init_path(s, px, py, (uint32_t)sample, J.seed);
+                    new_path(s, J.seed);
                     shadow_ray = false;
                     start_ray();
                 } else {
@@ -227,15 +242,24 @@ __global__ void __launch_bounds__(BLOCK) megakernel_persistent(const MkArgs a) {
     }
 
     // ---- fold counters: one atomic per warp ----
+    unsigned long long ext = n_ext, shd = n_shadow, steps = n_steps, prims = n_prims;
     for (int off = 16; off > 0; off >>= 1) {
-        n_ext += __shfl_down_sync(kFull, n_ext, off);
-        n_shadow += __shfl_down_sync(kFull, n_shadow, off);
+        ext += __shfl_down_sync(kFull, ext, off);
+        shd += __shfl_down_sync(kFull, shd, off);
         n_invalid += __shfl_down_sync(kFull, n_invalid, off);
+        if (COUNT) {
+            steps += __shfl_down_sync(kFull, steps, off);
+            prims += __shfl_down_sync(kFull, prims, off);
+        }
     }
     if (lane == 0) {
         if (a.count_rays) {
-            if (n_ext) atomicAdd(&a.counters->extension_rays, n_ext);
-            if (n_shadow) atomicAdd(&a.counters->shadow_rays, n_shadow);
+            if (ext) atomicAdd(&a.counters->extension_rays, ext);
+            if (shd) atomicAdd(&a.counters->shadow_rays, shd);
+            if (COUNT) {
+                atomicAdd(&a.counters->node_visits, steps);
+                atomicAdd(&a.counters->prim_tests, prims);
+            }
         }
         if (n_invalid) atomicAdd(&a.counters->invalid_hits, n_invalid);
     }
@@ -277,38 +301,54 @@ __global__ void film_commit_jobs(const JobDesc* jobs, const BatchHeader* hdr) {
         commit_pixel(J.film, J.lbuf, p, J.sample_count);
 }
 
-template <int BLOCK, bool MULTI>
+template <int BLOCK, bool MULTI, int MINB, bool COUNT>
 int resident_ctas(int blocks_per_sm) {
     int dev = 0, sms = 0, occ = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_persistent<BLOCK, MULTI>, BLOCK, 0),
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_persistent<BLOCK, MULTI, MINB, COUNT>,
+                                                             BLOCK, 0),
                "occupancy");
     if (blocks_per_sm > 0 && blocks_per_sm < occ) occ = blocks_per_sm;
     if (occ < 1) occ = 1;
     return sms * occ;
 }
 
-template <int BLOCK, bool MULTI>
+template <int BLOCK, bool MULTI, int MINB, bool COUNT>
 void launch_block(const MkArgs& args, long long units, int blocks_per_sm, cudaStream_t stream) {
-    long long grid = resident_ctas<BLOCK, MULTI>(blocks_per_sm);
+    long long grid = resident_ctas<BLOCK, MULTI, MINB, COUNT>(blocks_per_sm);
     if (units > 0) {
         const long long needed = (units + BLOCK - 1) / BLOCK;
         if (grid > needed) grid = needed;
     }
     if (grid < 1) grid = 1;
-    megakernel_persistent<BLOCK, MULTI><<<(unsigned)grid, BLOCK, 0, stream>>>(args);
+    megakernel_persistent<BLOCK, MULTI, MINB, COUNT><<<(unsigned)grid, BLOCK, 0, stream>>>(args);
     cuda_check(cudaGetLastError(), "megakernel launch");
+}
+
+// Dispatch over the compiled (block, occupancy) variants.
+template <bool MULTI, class F>
+auto dispatch(const MegakernelConfig& cfg, F&& f) {
+    if (cfg.block == 64) return f(std::integral_constant<int, 64>{}, std::integral_constant<int, 1>{});
+    if (cfg.block == 256) return f(std::integral_constant<int, 256>{}, std::integral_constant<int, 1>{});
+    if (cfg.block != 128) throw Error(WFB_ERR_INVALID_ARGUMENT, "megakernel block size must be 64, 128 or 256");
+    if (cfg.occupancy == 6) return f(std::integral_constant<int, 128>{}, std::integral_constant<int, 6>{});
+    if (cfg.occupancy == 8) return f(std::integral_constant<int, 128>{}, std::integral_constant<int, 8>{});
+    if (cfg.occupancy > 1) throw Error(WFB_ERR_INVALID_ARGUMENT, "megakernel occupancy target must be 0, 6 or 8");
+    return f(std::integral_constant<int, 128>{}, std::integral_constant<int, 1>{});
 }
 
 template <bool MULTI>
 void launch_any(const MkArgs& args, long long units, const MegakernelConfig& cfg, cudaStream_t stream) {
-    switch (cfg.block) {
-        case 64: launch_block<64, MULTI>(args, units, cfg.blocks_per_sm, stream); break;
-        case 256: launch_block<256, MULTI>(args, units, cfg.blocks_per_sm, stream); break;
-        case 128: launch_block<128, MULTI>(args, units, cfg.blocks_per_sm, stream); break;
-        default: throw Error(WFB_ERR_INVALID_ARGUMENT, "megakernel block size must be 64, 128 or 256");
+    if (args.count_rays) {  // counting runs use the instrumented 128-thread variant
+        launch_block<128, MULTI, 1, true>(args, units, cfg.blocks_per_sm, stream);
+        return;
     }
+    dispatch<MULTI>(cfg, [&](auto block, auto minb) {
+        launch_block<decltype(block)::value, MULTI, decltype(minb)::value, false>(args, units, cfg.blocks_per_sm,
+                                                                                  stream);
+        return 0;
+    });
 }
 
 }  // namespace
@@ -320,11 +360,10 @@ void launch_film_commit(const DevFilm& film, const float* lbuf, int count, cudaS
 }
 
 int megakernel_resident_threads(const MegakernelConfig& cfg) {
-    switch (cfg.block) {
-        case 64: return 64 * resident_ctas<64, false>(cfg.blocks_per_sm);
-        case 256: return 256 * resident_ctas<256, false>(cfg.blocks_per_sm);
-        default: return 128 * resident_ctas<128, false>(cfg.blocks_per_sm);
-    }
+    return dispatch<false>(cfg, [&](auto block, auto minb) {
+        return decltype(block)::value *
+               resident_ctas<decltype(block)::value, false, decltype(minb)::value, false>(cfg.blocks_per_sm);
+    });
 }
 
 int megakernel_split_chunks(int pixels, int sample_count, const MegakernelConfig& cfg) {

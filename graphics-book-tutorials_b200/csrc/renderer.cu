@@ -104,6 +104,8 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
     cuda_check(cudaMemcpy(&c, counters_, sizeof(c), cudaMemcpyDeviceToHost), "download counters");
     if (c.error != kErrNone)
         throw Error(WFB_ERR_DEVICE_WAIT, "a bounded device-side wait gave up; the render is incomplete");
+    last_node_visits_ = c.node_visits;
+    last_prim_tests_ = c.prim_tests;
     if (stats) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev0_, ev1_);
@@ -149,11 +151,13 @@ void Renderer::download(int spp_done, float* rgb, float* lum_var) {
 
 void Renderer::download_mean(int spp_done, float* rgb) { download(spp_done, rgb, nullptr); }
 
-void Renderer::configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight) {
+void Renderer::configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight,
+                         int occupancy) {
     if (block > 0) mk_cfg_.block = block;
-    if (blocks_per_sm > 0) mk_cfg_.blocks_per_sm = blocks_per_sm;
+    if (blocks_per_sm >= 0) mk_cfg_.blocks_per_sm = blocks_per_sm;
     if (min_active > 0) mk_cfg_.min_active = min_active;
-    if (split_chunks > 0) mk_cfg_.split_chunks = split_chunks;
+    if (split_chunks >= 0) mk_cfg_.split_chunks = split_chunks;
+    if (occupancy >= 0) mk_cfg_.occupancy = occupancy;
     if (mode_ == wf::GpuMode::Wavefront && (paths_in_flight > 0 || min_active > 0)) {
         if (paths_in_flight > 0) wf_cfg_.paths_in_flight = paths_in_flight;
         if (min_active > 0) wf_cfg_.min_active = min_active;

@@ -173,13 +173,14 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
     int item = -1;  // list position, -1: none
     uint32_t id = 0;  // slot (extend) or shadow record (shadow) of the current ray
     int node = -1;
-    wf::Vec3 o{0, 0, 0}, rd{0, 0, 1}, inv_d{0, 0, 1};
-    float tmin = 0.f;
+    wf::Vec3 o{0.f, 0.f, 0.f};
+    TravRay ray;
     wf::HitRecord h;
     h.t = 0.f;
     h.prim = -1;
     h.u = h.v = 0.f;
     bool exhausted = false;
+    unsigned n_prim_tests = 0;  // (the wavefront reports ray counts only)
     for (;;) {
         // refill lanes without a ray
         const bool need = item < 0 && !exhausted;
@@ -194,26 +195,12 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
                 if (i < n) {
                     item = (int)i;
                     id = SHADOW ? i : items[i];  // shadow records are numbered by queue position
-                    if (SHADOW) {
-                        const float4 d = P.sh_dir[id];
-                        const int slot = __float_as_int(P.sh_c[id].w);
-                        const float4 oo = P.ray_o[slot];
-                        o = wf::Vec3{oo.x, oo.y, oo.z};
-                        rd = wf::Vec3{d.x, d.y, d.z};
-                        tmin = wf::kRayEps;
-                        h.t = d.w;
-                    } else {
-                        const float4 oo = P.ray_o[id], d = P.ray_d[id];
-                        o = wf::Vec3{oo.x, oo.y, oo.z};
-                        tmin = oo.w;
-                        rd = wf::Vec3{d.x, d.y, d.z};
-                        h.t = d.w;
-                    }
-                    h.prim = -1;
-                    h.u = 0.0f;
-                    h.v = 0.0f;
-                    inv_d = wf::Vec3{1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
-                    node = s.n_nodes > 0 ? 0 : -1;
+                    // every ray starts at its path's origin with tmin = kRayEps (see TravRay)
+                    const int slot = SHADOW ? __float_as_int(P.sh_c[id].w) : (int)id;
+                    const float4 oo = P.ray_o[slot];
+                    const float4 d = SHADOW ? P.sh_dir[id] : P.ray_d[id];
+                    o = wf::Vec3{oo.x, oo.y, oo.z};
+                    traversal_begin(s.n_nodes, wf::Vec3{d.x, d.y, d.z}, d.w, &ray, &node, &h);
                 } else {
                     exhausted = true;
                 }
@@ -226,54 +213,7 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
             const unsigned tm = __ballot_sync(kFull, trav);
             if (tm == 0) break;
             if (__popc(tm) < a.min_active && __ballot_sync(kFull, !trav && !exhausted) != 0) break;
-            if (trav) {
-                const float4 na = __ldg(&s.nodes[2 * node]);
-                const float4 nb = __ldg(&s.nodes[2 * node + 1]);
-                const int skip = __float_as_int(na.w);
-                wf::Ray r;
-                r.o = o;
-                r.d = rd;
-                r.tmin = tmin;
-                r.tmax = h.t;
-                if (!wf::hit_box(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, r.o, inv_d, r.tmin, r.tmax)) {
-                    node = skip;
-                } else {
-                    const int leaf = __float_as_int(nb.w);
-                    if (leaf < 0) {
-                        node = node + 1;
-                    } else {
-                        node = skip;
-                        const int count = leaf & kLeafCountMask;
-                        const float4* rec = s.prims + 3 * (leaf >> kLeafCountBits);
-                        for (int i = 0; i < count; ++i, rec += 3) {
-                            const float4 q0 = __ldg(rec);
-                            const float4 q1 = __ldg(rec + 1);
-                            const int p = __float_as_int(q0.w);
-                            float t, u = 0.0f, v = 0.0f;
-                            bool hit;
-                            if (p < s.n_spheres) {
-                                hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
-                            } else {
-                                const float4 q2 = __ldg(rec + 2);
-                                hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
-                                                            wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
-                            }
-                            if (hit) {
-                                r.tmax = t;
-                                h.t = t;
-                                h.prim = p;
-                                h.u = u;
-                                h.v = v;
-                                if (SHADOW) {
-                                    node = -1;
-                                    break;
-                                }
-                            }
-                        }
-                    }
-                }
-                if (node >= s.n_nodes) node = -1;
-            }
+            if (trav) traversal_step(s.nodes, s.prims, s.n_nodes, s.n_spheres, o, ray, SHADOW, node, h, n_prim_tests);
         }
         // retire finished rays
         if (item >= 0 && node < 0) {

@@ -92,6 +92,11 @@ int wfb_scene_export(wfb_scene_t scene, void* spheres, float* vertices, int* tri
                      void* materials, void* nodes, int* prim_order, void* lights);
 /* Replaces wf::scene_hash (WVM/src/scene.cpp:107-160). */
 uint64_t wfb_scene_hash(wfb_scene_t scene);
+/* Rebuilds the BVH of a scene not yet uploaded, with SAH knobs: bins (8 = reference-compatible
+ * policy), leaves of at most max_leaf primitives (1..15), traversal_cost relative to one
+ * primitive test. Replaces wf::build_bvh (WVM/src/bvh_build.cpp:228-251) for tuning; the tree
+ * stays in the preorder skip-link layout. */
+int wfb_scene_rebuild_bvh(wfb_scene_t scene, int bins, int max_leaf, float traversal_cost);
 /* Replaces wf::validate_bvh (WVM/src/bvh_build.cpp:253-323): writes "" when valid. */
 int wfb_scene_validate_bvh(wfb_scene_t scene, char* msg, int len);
 /* Releases the caller's reference; device arrays live until the last renderer using them is gone. */
@@ -118,7 +123,9 @@ typedef struct {
     int64_t invalid_hits;
     uint64_t peak_vram_bytes;
     double stage_ms[8]; /* extend, classify, lambert, metal, dielectric, shadow, compact, other */
-} wfb_render_stats; /* wf::RenderStats (WVM/include/wf/renderer.hpp:23-37) */
+    uint64_t node_visits; /* megakernel, with count_rays: BVH nodes visited (box tests) */
+    uint64_t prim_tests;  /* megakernel, with count_rays: primitive intersection tests */
+} wfb_render_stats; /* wf::RenderStats (WVM/include/wf/renderer.hpp:23-37) plus traversal counts */
 
 /* GpuRenderer(const Scene&, GpuMode) (WVM/src/gpu/gpu_renderer.cu:100-238). */
 int wfb_renderer_create(wfb_scene_t scene, int mode, wfb_renderer_t* out);
@@ -144,12 +151,13 @@ int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render
                         float* rgb, float* lum_var);
 /* GpuRenderer::device_bytes (WVM/src/gpu/gpu_renderer.cu:366-377). */
 uint64_t wfb_renderer_device_bytes(wfb_renderer_t r);
-/* Launch configuration knobs (no reference counterpart; set by the autotuner). Any value <= 0
- * keeps the current setting. Megakernel: block 64/128/256 threads, CTAs per SM, the minimum
- * number of traversing lanes per warp before shading runs (1..32), work units per pixel.
- * Wavefront: block, paths in flight. */
+/* Launch configuration knobs (no reference counterpart; set by the autotuner). Any value < 0
+ * keeps the current setting. Megakernel: block 64/128/256 threads, CTAs per SM (0: all that fit),
+ * the minimum number of traversing lanes per warp before shading runs (1..32), work units per
+ * pixel (0: automatic), occupancy target (block 128: 0 none, 6 or 8 CTAs per SM by a register
+ * cap). Wavefront: paths in flight and min_active. */
 int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int min_active,
-                           int split_chunks, int paths_in_flight);
+                           int split_chunks, int paths_in_flight, int occupancy);
 int wfb_renderer_width(wfb_renderer_t r);
 int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */
