@@ -96,15 +96,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def read_profile_traffic():
-    """DRAM bytes per path sample of the megakernel from the committed ncu summary, if present."""
+def read_profile():
+    """`key: number` lines of the committed ncu summary of the megakernel (issue activity, lanes per
+    instruction, DRAM bytes of a full-size launch), or {} if absent."""
     path = os.path.join(PROFILE_DIR, "megakernel_icospheres.txt")
+    out = {}
     if not os.path.exists(path):
-        return None
+        return out
     for line in open(path):
-        if line.startswith("dram_bytes_per_sample:"):
-            return float(line.split(":", 1)[1])
-    return None
+        key, sep, val = line.partition(":")
+        if sep and key and " " not in key.strip():
+            try:
+                out[key.strip()] = float(val)
+            except ValueError:
+                pass
+    return out
 
 
 def measured_peaks():
@@ -278,7 +284,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--arm", default="megakernel", choices=["megakernel", "wavefront"])
+    ap.add_argument("--arm", default="auto", choices=["auto", "megakernel", "wavefront"],
+                    help="auto: the autotuner picks the arm and its launch knobs (untimed, before warm-up)")
+    ap.add_argument("--no-tune", action="store_true", help="library default knobs (megakernel unless --arm)")
     ap.add_argument("--ref-spp", type=int, default=2, help="samples per pixel of one reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -319,10 +327,21 @@ def main():
         if dist is not None:
             dist.destroy_process_group()
         return
-    mode = wfb.MEGAKERNEL if args.arm == "megakernel" else wfb.WAVEFRONT
     scene = wfb.Scene.generate(SCENE, WIDTH, HEIGHT, SEED, 16)
     host_arrays = scene.export()
+    tuning = None
+    if not args.no_tune:
+        # Untimed: measured probe renders of both arms pick the arm and its launch knobs.
+        tuning = wfb.autotune(scene, WIDTH, HEIGHT, probe_spp=2, max_depth=DEPTH,
+                              try_wavefront=args.arm in ("auto", "wavefront"))
+    if args.arm == "auto":
+        mode = tuning.mode if tuning is not None else wfb.MEGAKERNEL
+    else:
+        mode = wfb.MEGAKERNEL if args.arm == "megakernel" else wfb.WAVEFRONT
+    arm = "megakernel" if mode == wfb.MEGAKERNEL else "wavefront"
     renderer = wfb.GpuRenderer(scene, mode)
+    if tuning is not None:
+        renderer.apply_tuning(tuning)
     params = wfb.RenderParams(spp=SPP, seed=SEED, max_depth=DEPTH)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
@@ -341,12 +360,14 @@ def main():
     torch.cuda.synchronize()
     clocks.start()
     dev_ms = []
+    launches = 0
     for _ in range(args.steps):
         flush.zero_()  # L2 flush outside the event-timed region
         torch.cuda.synchronize()
         st = wfb.RenderStats()
         img = renderer.render(params, st)  # render_ms: CUDA events on the launching stream
         dev_ms.append(st.render_ms)
+        launches += st.kernel_launches
     torch.cuda.synchronize()
     clk = clocks.stop()
     total_ms = float(sum(dev_ms))
@@ -367,6 +388,9 @@ def main():
         t0 = time.perf_counter()
         s2 = wfb.Scene.from_arrays(host_arrays)
         r2 = wfb.GpuRenderer(s2, mode)
+        if tuning is not None:  # served from the tuner's cache (same scene hash and size)
+            r2.apply_tuning(wfb.autotune(s2, WIDTH, HEIGHT, probe_spp=2, max_depth=DEPTH,
+                                         try_wavefront=args.arm in ("auto", "wavefront")))
         out = r2.render(params)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
@@ -387,25 +411,29 @@ def main():
     peaks, peak_kind = measured_peaks()
     bytes_per_sample = 224.0 * ext_ps + 96.0 * sh_ps + 40.0
     achieved = samples * bytes_per_sample / (ms_per_step / 1e3) / 1e9
-    traffic_ps = read_profile_traffic()
+    prof = read_profile()
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "arm": args.arm, "parallelism": f"replicas{world}" if world > 1 else "1gpu",
+        "config": {"workload": WORKLOAD, "arm": arm, "tuning": tuning.as_dict() if tuning else "library defaults",
+                   "parallelism": f"replicas{world}" if world > 1 else "1gpu",
                    "l2": "flushed (256 MB write) before every timed step", "scene_hash": "%016x" % scene.hash()},
         "roofline": {
             "bound": "hbm", "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": round(achieved / peaks["hbm_gbs"], 4),
-            "traffic": round(traffic_ps * samples) if traffic_ps else None,
+            "traffic": int(prof["dram_bytes_per_launch_full"]) if "dram_bytes_per_launch_full" in prof else None,
             "peak_source": peak_kind,
             "bytes_model": "224*ext + 96*shadow + 40 B per sample (path-state bytes a wavefront moves)",
             "ext_rays_per_sample": round(ext_ps, 4), "shadow_rays_per_sample": round(sh_ps, 4),
-            "kernel": "megakernel_persistent" if args.arm == "megakernel" else "wavefront_persistent",
+            "kernel": "megakernel_persistent" if arm == "megakernel" else "wavefront_persistent",
+            "issue_active_frac": prof.get("issue_active_frac"),
+            "lanes_per_instr": prof.get("lanes_per_instr"),
+            "note": "traversal is issue-bound on an L2-resident BVH; see issue_active_frac x lanes_per_instr/32",
         },
         "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": args.steps,
+        "gpu_launches": launches,
         "mrays_per_s": round((ext_ps + sh_ps) * value, 2),
         "clocks": clk,
         "device": wfb.device_name(),

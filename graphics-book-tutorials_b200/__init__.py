@@ -93,11 +93,19 @@ class _CRenderStats(ctypes.Structure):
                 ("queue_high_water", ctypes.c_int64 * 5), ("queue_overflows", ctypes.c_int64),
                 ("invalid_hits", ctypes.c_int64), ("peak_vram_bytes", ctypes.c_uint64),
                 ("stage_ms", ctypes.c_double * 8), ("node_visits", ctypes.c_uint64),
-                ("prim_tests", ctypes.c_uint64)]
+                ("prim_tests", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64)]
 
 
 STAGE_NAMES = ("extend", "classify", "shade_lambert", "shade_metal", "shade_dielectric", "shadow",
                "compact", "other")
+
+
+class _CTuneResult(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("block", ctypes.c_int), ("occupancy", ctypes.c_int),
+                ("min_active", ctypes.c_int), ("paths_in_flight", ctypes.c_int), ("wf_min_active", ctypes.c_int),
+                ("msamples_s", ctypes.c_double),
+                ("megakernel_msamples_s", ctypes.c_double), ("wavefront_msamples_s", ctypes.c_double),
+                ("candidates", ctypes.c_int)]
 
 
 @dataclass
@@ -131,13 +139,14 @@ class RenderStats:
     stages: dict = field(default_factory=dict)
     node_visits: int = 0  # megakernel with count_rays: BVH nodes visited
     prim_tests: int = 0   # megakernel with count_rays: primitive tests
+    kernel_launches: int = 0  # kernels of the library launched by the call
 
     @classmethod
     def _from_c(cls, c: _CRenderStats) -> "RenderStats":
         return cls(c.render_ms, c.total_ms, int(c.extension_rays), int(c.shadow_rays),
                    [int(v) for v in c.queue_high_water], int(c.queue_overflows), int(c.invalid_hits),
                    int(c.peak_vram_bytes), {n: float(c.stage_ms[i]) for i, n in enumerate(STAGE_NAMES)},
-                   int(c.node_visits), int(c.prim_tests))
+                   int(c.node_visits), int(c.prim_tests), int(c.kernel_launches))
 
 
 @dataclass
@@ -199,6 +208,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_compact_u32": (i32, [vp, vp, vp, vp, vp, i32, vp, vp]),
         "wfb_test_queue_push": (i32, [vp, i32, vp, u32, vp, vp, vp]),
         "wfb_scan_workspace_check": (i32, [vp, vp]),
+        "wfb_autotune": (i32, [vp, i32, i32, i32, i32, i32, ctypes.POINTER(_CTuneResult)]),
+        "wfb_renderer_apply_tuning": (i32, [vp, ctypes.POINTER(_CTuneResult)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -386,6 +397,10 @@ class GpuRenderer:
         _check(load_library().wfb_renderer_configure(self._h, block, blocks_per_sm, min_active, split_chunks,
                                                       paths_in_flight, occupancy))
 
+    def apply_tuning(self, tuning: "TuneResult") -> None:
+        """Applies the knobs of an autotune result that belong to this renderer's arm."""
+        _check(load_library().wfb_renderer_apply_tuning(self._h, ctypes.byref(tuning._c)))
+
     def close(self) -> None:
         if self._h is not None and self._h.value:
             load_library().wfb_renderer_destroy(self._h)
@@ -396,6 +411,41 @@ class GpuRenderer:
             self.close()
         except Exception:
             pass
+
+
+@dataclass
+class TuneResult:
+    """Outcome of :func:`autotune`: the faster arm, the best knobs of each arm, measured rates."""
+    mode: int
+    block: int
+    occupancy: int
+    min_active: int
+    paths_in_flight: int
+    wf_min_active: int
+    msamples_s: float
+    megakernel_msamples_s: float
+    wavefront_msamples_s: float
+    candidates: int
+    _c: _CTuneResult = field(repr=False, default=None)
+
+    def as_dict(self) -> dict:
+        return {"arm": "megakernel" if self.mode == MEGAKERNEL else "wavefront",
+                "megakernel": {"block": self.block, "occupancy": self.occupancy, "min_active": self.min_active},
+                "wavefront": {"paths_in_flight": self.paths_in_flight, "min_active": self.wf_min_active},
+                "msamples_s": round(self.msamples_s, 2),
+                "megakernel_msamples_s": round(self.megakernel_msamples_s, 2),
+                "wavefront_msamples_s": round(self.wavefront_msamples_s, 2), "candidates": self.candidates}
+
+
+def autotune(scene: Scene, width: int, height: int, probe_spp: int = 2, max_depth: int = 8,
+             try_wavefront: bool = True) -> TuneResult:
+    """Measures launch configurations of both arms on the scene's camera at width x height and returns the
+    fastest; cached per scene hash and size inside the library (wfb_autotune)."""
+    c = _CTuneResult()
+    _check(load_library().wfb_autotune(scene.handle, int(width), int(height), int(probe_spp), int(max_depth),
+                                       1 if try_wavefront else 0, ctypes.byref(c)))
+    return TuneResult(c.mode, c.block, c.occupancy, c.min_active, c.paths_in_flight, c.wf_min_active, c.msamples_s,
+                      c.megakernel_msamples_s, c.wavefront_msamples_s, c.candidates, c)
 
 
 def compare_results(a: RenderResult, b: RenderResult) -> dict:

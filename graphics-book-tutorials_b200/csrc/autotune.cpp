@@ -1,0 +1,110 @@
+// Autotuner: picks the arm (megakernel or wavefront) and its launch knobs per scene and
+// resolution from measured runs on the current GPU.
+//
+// Candidates are rendered for `probe_spp` samples at the target resolution, each once to warm up
+// and once timed with CUDA events; the fastest measured configuration wins. Every candidate
+// renders the same film bits (launch knobs never change the arithmetic), so tuning is purely a
+// speed decision. Results are cached per (scene hash, width, height, probe_spp, max_depth).
+// The result holds the best knobs of each arm, so a renderer of either arm can apply it.
+//   megakernel: (block, occupancy target) in {(128,8), (128,6), (128,0), (64,0), (256,0)} x
+//               min_active in {8, 16, 20, 24, 28}
+//   wavefront:  paths in flight in {512K, 1M, 2M} x min_active {16, 24}; its queues are sized to
+//               the pool, so they never drop a path.
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include "autotune.hpp"
+#include "../../include/wfb200.h"
+
+namespace wfb {
+namespace {
+
+using Key = std::tuple<uint64_t, int, int, int, int, bool>;
+std::mutex g_mu;
+std::map<Key, TuneResult> g_cache;
+
+double measure(Renderer& r, const PassParams& p) {
+    r.reset();
+    r.run_passes(p, nullptr);  // warm-up (module load, pool allocation)
+    r.reset();
+    wf::RenderStats st{};
+    r.run_passes(p, &st);
+    return st.render_ms;
+}
+
+}  // namespace
+
+TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camera& cam, int width, int height,
+                    int probe_spp, int max_depth, bool try_wavefront) {
+    if (!scene) throw Error(WFB_ERR_INVALID_ARGUMENT, "null scene");
+    if (width <= 0 || height <= 0 || probe_spp <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "bad tuning size");
+    const Key key{wf::scene_hash(scene->host), width, height, probe_spp, max_depth, try_wavefront};
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        auto it = g_cache.find(key);
+        if (it != g_cache.end()) return it->second;
+    }
+    PassParams p;
+    p.first_sample = 0;
+    p.sample_count = probe_spp;
+    p.seed = 1234;
+    p.max_depth = max_depth;
+    const double samples = (double)width * height * probe_spp;
+    TuneResult best;
+    best.mode = WFB_MODE_MEGAKERNEL;
+    double mk_ms = 1e300, wf_ms = 1e300;
+    {
+        Renderer r(scene, wf::GpuMode::Megakernel);
+        r.set_camera(cam, width, height);
+        const int shapes[][2] = {{128, 8}, {128, 6}, {128, 0}, {64, 0}, {256, 0}};
+        const int actives[] = {8, 16, 20, 24, 28};
+        for (const auto& sh : shapes)
+            for (int ma : actives) {
+                r.configure(sh[0], 0, ma, 0, -1, sh[1]);
+                const double ms = measure(r, p);
+                best.candidates++;
+                if (ms < mk_ms) {
+                    mk_ms = ms;
+                    best.block = sh[0];
+                    best.occupancy = sh[1];
+                    best.min_active = ma;
+                }
+            }
+    }
+    if (try_wavefront) {
+        const int pools[] = {1 << 19, 1 << 20, 1 << 21};
+        const int actives[] = {16, 24};
+        Renderer r(scene, wf::GpuMode::Wavefront);
+        r.set_camera(cam, width, height);
+        for (int pool : pools)
+            for (int ma : actives) {
+                r.configure(-1, -1, ma, -1, pool, -1);
+                const double ms = measure(r, p);
+                best.candidates++;
+                if (ms < wf_ms) {
+                    wf_ms = ms;
+                    best.paths_in_flight = pool;
+                    best.wf_min_active = ma;
+                }
+            }
+    }
+    best.megakernel_msamples_s = samples / mk_ms / 1e3;
+    if (try_wavefront) best.wavefront_msamples_s = samples / wf_ms / 1e3;
+    best.mode = wf_ms < mk_ms ? WFB_MODE_WAVEFRONT : WFB_MODE_MEGAKERNEL;
+    best.msamples_s = samples / std::min(mk_ms, wf_ms) / 1e3;
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_cache[key] = best;
+    return best;
+}
+
+void apply_tuning(Renderer& r, const TuneResult& t) {
+    if (r.mode() == wf::GpuMode::Megakernel)
+        r.configure(t.block > 0 ? t.block : -1, -1, t.min_active > 0 ? t.min_active : -1, -1, -1,
+                    t.occupancy >= 0 ? t.occupancy : -1);
+    else
+        r.configure(-1, -1, t.wf_min_active > 0 ? t.wf_min_active : -1, -1,
+                    t.paths_in_flight > 0 ? t.paths_in_flight : -1, -1);
+}
+
+}  // namespace wfb

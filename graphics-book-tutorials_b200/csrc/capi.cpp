@@ -5,6 +5,7 @@
 #include <mutex>
 #include <string>
 #include "engine.hpp"
+#include "autotune.hpp"
 #include "noalloc.hpp"
 #include "queues.hpp"
 #include "server.hpp"
@@ -111,6 +112,7 @@ void to_c_stats(const wf::RenderStats& s, wfb_render_stats* out) {
     for (int i = 0; i < 8; ++i) out->stage_ms[i] = st[i];
     out->node_visits = 0;
     out->prim_tests = 0;
+    out->kernel_launches = 0;
 }
 
 void need(bool ok, const char* msg) {
@@ -134,6 +136,27 @@ int wfb_device_name(char* buf, int len) {
         wfb::cuda_check(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
         std::strncpy(buf, prop.name, (size_t)len - 1);
         buf[len - 1] = '\0';
+    });
+}
+
+int wfb_device_facts_get(wfb_device_facts* out) {
+    return guarded([&] {
+        need(out != nullptr, "null argument");
+        int dev = 0;
+        wfb::cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        cudaDeviceProp prop;
+        wfb::cuda_check(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+        size_t free_b = 0, total_b = 0;
+        wfb::cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+        std::memset(out, 0, sizeof(*out));
+        std::strncpy(out->name, prop.name, sizeof(out->name) - 1);
+        cudaDriverGetVersion(&out->driver_version);
+        cudaRuntimeGetVersion(&out->runtime_version);
+        out->cc_major = prop.major;
+        out->cc_minor = prop.minor;
+        out->sm_count = prop.multiProcessorCount;
+        out->total_memory_bytes = total_b;
+        out->free_memory_bytes = free_b;
     });
 }
 
@@ -300,6 +323,7 @@ int wfb_renderer_run_passes(wfb_renderer_t r, int first_sample, int count, const
             to_c_stats(st, stats);
             stats->node_visits = r->r->last_node_visits();
             stats->prim_tests = r->r->last_prim_tests();
+            stats->kernel_launches = (uint64_t)r->r->last_kernel_launches();
         }
     });
 }
@@ -338,6 +362,7 @@ int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render
             to_c_stats(st, stats);
             stats->node_visits = r->r->last_node_visits();
             stats->prim_tests = r->r->last_prim_tests();
+            stats->kernel_launches = (uint64_t)r->r->last_kernel_launches();
         }
     });
 }
@@ -361,6 +386,40 @@ int wfb_renderer_height(wfb_renderer_t r) { return r ? r->r->height() : 0; }
 int wfb_renderer_destroy(wfb_renderer_t r) {
     delete r;
     return WFB_OK;
+}
+
+int wfb_autotune(wfb_scene_t scene, int width, int height, int probe_spp, int max_depth, int try_wavefront,
+                 wfb_tune_result* out) {
+    return guarded([&] {
+        need(scene && out, "null argument");
+        if (scene->host.nodes.empty()) throw wfb::Error(WFB_ERR_NOT_FINALIZED, "Scene not finalized (no BVH nodes)");
+        const wfb::TuneResult t = wfb::autotune(scene->get_resident(), scene->host.camera, width, height, probe_spp,
+                                                max_depth, try_wavefront != 0);
+        out->mode = t.mode;
+        out->block = t.block;
+        out->occupancy = t.occupancy;
+        out->min_active = t.min_active;
+        out->paths_in_flight = t.paths_in_flight;
+        out->wf_min_active = t.wf_min_active;
+        out->msamples_s = t.msamples_s;
+        out->megakernel_msamples_s = t.megakernel_msamples_s;
+        out->wavefront_msamples_s = t.wavefront_msamples_s;
+        out->candidates = t.candidates;
+    });
+}
+
+int wfb_renderer_apply_tuning(wfb_renderer_t r, const wfb_tune_result* t) {
+    return guarded([&] {
+        need(r && t, "null argument");
+        wfb::TuneResult tr;
+        tr.mode = t->mode;
+        tr.block = t->block;
+        tr.occupancy = t->occupancy;
+        tr.min_active = t->min_active;
+        tr.paths_in_flight = t->paths_in_flight;
+        tr.wf_min_active = t->wf_min_active;
+        wfb::apply_tuning(*r->r, tr);
+    });
 }
 
 int wfb_batch_create(int max_jobs, int use_graph, int block, int min_active, wfb_batch_t* out) {
@@ -401,7 +460,10 @@ int wfb_batch_run(wfb_batch_t b, int count_rays, wfb_render_stats* stats) {
         need(b != nullptr, "null batch");
         wf::RenderStats st{};
         b->b->run(count_rays != 0, &st);
-        if (stats) to_c_stats(st, stats);
+        if (stats) {
+            to_c_stats(st, stats);
+            stats->kernel_launches = 2;  // persistent megakernel over the job table + film commit
+        }
     });
 }
 

@@ -62,9 +62,10 @@ int megakernel_resident_threads(const MegakernelConfig& cfg);
 int megakernel_split_chunks(int pixels, int sample_count, const MegakernelConfig& cfg);
 // Adds samples [first, first + count) of every pixel to `film`. With chunks > 1, `lbuf` must hold
 // 3 * pixels * count floats (per-sample radiance, committed in sample order after the kernel).
-void launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters,
+// Returns the number of kernels launched.
+int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters,
                        unsigned int* work_counter, float* lbuf, const PassParams& p,
-                       const MegakernelConfig& cfg, int chunks, cudaStream_t stream);
+                      const MegakernelConfig& cfg, int chunks, cudaStream_t stream);
 
 // Adds per-(pixel, sample) radiance slots (3 floats, pixel-major, `count` samples per pixel) to the
 // film sums in ascending sample order (megakernel.cu).
@@ -119,6 +120,8 @@ public:
     // Traversal counts of the last run_passes with count_rays (megakernel only).
     uint64_t last_node_visits() const { return last_node_visits_; }
     uint64_t last_prim_tests() const { return last_prim_tests_; }
+    // Kernels of this library launched by the last run_passes.
+    int last_kernel_launches() const { return last_launches_; }
     // Reference download convention (WVM/src/gpu/gpu_renderer.cu:306-341).
     void download(int spp_done, float* rgb, float* lum_var);
     void download_mean(int spp_done, float* rgb);
@@ -151,6 +154,7 @@ private:
     MegakernelConfig mk_cfg_{};
     WavefrontConfig wf_cfg_{};
     uint64_t last_node_visits_ = 0, last_prim_tests_ = 0;
+    int last_launches_ = 0;
     struct Wavefront;
     std::unique_ptr<Wavefront> wf_;
 };

@@ -394,10 +394,10 @@ JobDesc make_job(const DevScene& s, const DevFilm& film, float* lbuf, int first_
     return j;
 }
 
-void launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters, unsigned int* work_counter,
-                       float* lbuf, const PassParams& p, const MegakernelConfig& cfg, int chunks,
-                       cudaStream_t stream) {
-    if (p.sample_count <= 0 || film.pixels <= 0) return;
+int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters, unsigned int* work_counter,
+                      float* lbuf, const PassParams& p, const MegakernelConfig& cfg, int chunks,
+                      cudaStream_t stream) {
+    if (p.sample_count <= 0 || film.pixels <= 0) return 0;
     if (chunks > 1 && lbuf == nullptr) throw Error(WFB_ERR_INTERNAL, "split megakernel needs a sample buffer");
     MkArgs args{};
     args.job0 = make_job(s, film, lbuf, p.first_sample, p.sample_count, chunks, p.seed, p.max_depth);
@@ -409,7 +409,11 @@ void launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* coun
     args.min_active = cfg.min_active;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
     launch_any<false>(args, args.job0.units, cfg, stream);
-    if (args.job0.chunks > 1) launch_film_commit(film, lbuf, p.sample_count, stream);
+    if (args.job0.chunks > 1) {
+        launch_film_commit(film, lbuf, p.sample_count, stream);
+        return 2;
+    }
+    return 1;
 }
 
 void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, int max_jobs, DevCounters* counters,

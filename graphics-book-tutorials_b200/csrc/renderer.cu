@@ -94,9 +94,9 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
                 lbuf_floats_ = need;
             }
         }
-        launch_megakernel(view_, film_, counters_, work_, lbuf_, p, mk_cfg_, chunks, stream_);
+        last_launches_ = launch_megakernel(view_, film_, counters_, work_, lbuf_, p, mk_cfg_, chunks, stream_);
     } else {
-        wf_->engine.run(view_, film_, counters_, p, stats ? &stats->stages : nullptr, stream_);
+        last_launches_ = wf_->engine.run(view_, film_, counters_, p, stats ? &stats->stages : nullptr, stream_);
     }
     cuda_check(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
     cuda_check(cudaEventSynchronize(ev1_), "render");

@@ -588,9 +588,9 @@ WavefrontEngine::~WavefrontEngine() {
 
 uint64_t WavefrontEngine::bytes() const { return bytes_ + (state_ ? state_->lbuf_floats * sizeof(float) : 0); }
 
-void WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
-                          wf::StageTimes* stages, cudaStream_t stream) {
-    if (p.sample_count <= 0 || film.pixels <= 0) return;
+int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
+                         wf::StageTimes* stages, cudaStream_t stream) {
+    if (p.sample_count <= 0 || film.pixels <= 0) return 0;
     State& st = *state_;
     WfArgs a;
     a.s = s;
@@ -648,6 +648,7 @@ void WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* c
         stages->compact += ns[6] * 1e-6;
         stages->other += ns[7] * 1e-6;
     }
+    return a.chunks > 1 ? 4 : 3;
 }
 
 }  // namespace wfb

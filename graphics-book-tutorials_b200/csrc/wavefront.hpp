@@ -14,8 +14,9 @@ public:
     WavefrontEngine(const WavefrontEngine&) = delete;
     WavefrontEngine& operator=(const WavefrontEngine&) = delete;
 
-    // Adds samples [p.first_sample, p.first_sample + p.sample_count) of every pixel to `film`.
-    void run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
+    // Adds samples [p.first_sample, p.first_sample + p.sample_count) of every pixel to `film`;
+    // returns the number of kernels launched.
+    int run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
              wf::StageTimes* stages, cudaStream_t stream);
     uint64_t bytes() const;
     int capacity() const { return capacity_; }

@@ -1,6 +1,6 @@
 // C++ renderer interface: the reference's GpuRenderer class (WVM/include/wf/renderer.hpp:11-74),
 // declared identically so code written against the reference (its CLI, its GPU tests) links
-// against this engine. The implementation (csrc/gpu_renderer_shim.cpp) forwards every call to
+// against this engine. The implementation (shim/gpu_renderer_shim.cpp, built as libwf_gpu.so) forwards every call to
 // the engine's C ABI (include/wfb200.h).
 #pragma once
 #include <cstdint>

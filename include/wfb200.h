@@ -49,6 +49,16 @@ int wfb_abi_version(void);
 const char* wfb_last_error(void);
 /* Writes the CUDA device name; replaces wf::GpuRenderer::device_name (WVM/src/gpu/gpu_renderer.cu:379-390). */
 int wfb_device_name(char* buf, int len);
+/* Facts of the current CUDA device; replaces wf::query_cuda_device (WVM/src/gpu/gpu_renderer.cu:13-56). */
+typedef struct {
+    char name[256];
+    int driver_version;  /* cudaDriverGetVersion, e.g. 12090 */
+    int runtime_version; /* cudaRuntimeGetVersion of this library */
+    int cc_major, cc_minor;
+    int sm_count;
+    uint64_t total_memory_bytes, free_memory_bytes;
+} wfb_device_facts;
+int wfb_device_facts_get(wfb_device_facts* out);
 
 /* ---- scenes ---------------------------------------------------------------------------------
  * Host description of a scene in the reference layouts. n_nodes == 0 means "not finalized". */
@@ -125,6 +135,7 @@ typedef struct {
     double stage_ms[8]; /* extend, classify, lambert, metal, dielectric, shadow, compact, other */
     uint64_t node_visits; /* megakernel, with count_rays: BVH nodes visited (box tests) */
     uint64_t prim_tests;  /* megakernel, with count_rays: primitive intersection tests */
+    uint64_t kernel_launches; /* kernels of this library launched by the call */
 } wfb_render_stats; /* wf::RenderStats (WVM/include/wf/renderer.hpp:23-37) plus traversal counts */
 
 /* GpuRenderer(const Scene&, GpuMode) (WVM/src/gpu/gpu_renderer.cu:100-238). */
@@ -162,6 +173,23 @@ int wfb_renderer_width(wfb_renderer_t r);
 int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */
 int wfb_renderer_destroy(wfb_renderer_t r);
+
+/* ---- autotuner (no reference counterpart) ------------------------------------------------------
+ * Measures launch configurations of both arms on `scene` (its camera) at width x height for
+ * probe_spp samples: the faster arm (mode), the best megakernel block / occupancy target /
+ * min_active and the best wavefront paths in flight / min_active (0 when the wavefront was not
+ * tried). Cached per scene hash and size. */
+typedef struct {
+    int mode;
+    int block, occupancy, min_active;
+    int paths_in_flight, wf_min_active;
+    double msamples_s, megakernel_msamples_s, wavefront_msamples_s;
+    int candidates;
+} wfb_tune_result;
+int wfb_autotune(wfb_scene_t scene, int width, int height, int probe_spp, int max_depth, int try_wavefront,
+                 wfb_tune_result* out);
+/* Applies the knobs of a tuning result that belong to the renderer's arm. */
+int wfb_renderer_apply_tuning(wfb_renderer_t r, const wfb_tune_result* t);
 
 /* ---- batched rendering (no reference counterpart: one scene/camera/job per GpuRenderer) -------
  * Many jobs of uneven size rendered in ONE persistent launch, replayed through a CUDA graph
