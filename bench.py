@@ -121,24 +121,18 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def dist_setup(n_gpus):
-    if n_gpus <= 1 and "WORLD_SIZE" not in os.environ:
-        return None, 0, 1, 0
-    import torch.distributed as dist
-    import datetime
-    rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", 1))
-    local = int(os.environ.get("LOCAL_RANK", 0))
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    return dist, rank, world, local
+def load_replicas():
+    spec = importlib.util.spec_from_file_location("wfb200_replicas", os.path.join(PKG_DIR, "replicas.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def run_reference(args):
     """Reference CPU arm (render_cpu compiled from the reference sources) on this host's cores."""
-    dist, rank, world, _ = dist_setup(args.gpus)
+    # Rank 0 alone times the CPU arm; the other ranks exit without work (no process group needed).
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
         return
     orc = load_oracle()
     wfb = load_engine()
@@ -170,8 +164,6 @@ def run_reference(args):
         "e2e": {"value": round(value, 4), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
 
 
 def cpu_baseline(wfb, seconds_target=12.0):
@@ -309,9 +301,12 @@ def main():
         run_reference(args)
         return
 
-    dist, rank, world, local = dist_setup(args.gpus)
     import torch
+    rep = load_replicas()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    group = rep.ReplicaGroup("nccl", device=f"cuda:{local}")
+    rank, world = group.rank, group.world
     wfb = load_engine()
     if args.mode in ("batch", "serve"):
         scenes = mix_scenes(wfb)
@@ -324,8 +319,7 @@ def main():
                 for plain in (False, True):
                     r = bench_serve(wfb, scenes, lam, args.duration, plain=plain)
                     print(json.dumps({"mode": "serve", **r}), flush=True)
-        if dist is not None:
-            dist.destroy_process_group()
+        group.close()
         return
     scene = wfb.Scene.generate(SCENE, WIDTH, HEIGHT, SEED, 16)
     host_arrays = scene.export()
@@ -355,8 +349,7 @@ def main():
         flush.zero_()
         renderer.render(params)
     clocks = ClockSampler(torch.cuda.current_device())
-    if dist is not None:
-        dist.barrier()
+    group.barrier()
     torch.cuda.synchronize()
     clocks.start()
     dev_ms = []
@@ -370,14 +363,10 @@ def main():
         launches += st.kernel_launches
     torch.cuda.synchronize()
     clk = clocks.stop()
-    total_ms = float(sum(dev_ms))
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
+    total_ms = group.max(float(sum(dev_ms)))  # the job takes as long as its slowest replica
+    group.barrier()
     assert np.array_equal(img.rgb.view(np.uint32), ref_img.rgb.view(np.uint32)), "render is not deterministic"
-    value = samples * args.steps * world / (total_ms / 1e3) / 1e6
+    value = rep.whole_job_rate(samples, args.steps, world, total_ms / 1e3) / 1e6
     ms_per_step = total_ms / args.steps
 
     # e2e through the public API: host arrays -> scene upload -> render -> film back in host memory
@@ -401,12 +390,8 @@ def main():
         s2.close()
     e2e_value = None
     if e2e_times:
-        e2e_s = sum(e2e_times) / len(e2e_times)
-        if dist is not None:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e_value = round(samples * world / e2e_s / 1e6, 3)
+        e2e_s = group.max(sum(e2e_times) / len(e2e_times))
+        e2e_value = round(rep.whole_job_rate(samples, 1, world, e2e_s) / 1e6, 3)
 
     peaks, peak_kind = measured_peaks()
     bytes_per_sample = 224.0 * ext_ps + 96.0 * sh_ps + 40.0
@@ -447,8 +432,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     del flush
-    if dist is not None:
-        dist.destroy_process_group()
+    group.close()
 
 
 if __name__ == "__main__":

@@ -142,7 +142,7 @@ def summarise(path: str) -> dict:
 
 def short_name(kernel: str) -> str:
     """`void ns::<unnamed>::k<128, 0, 8, 0>(ns::Args)` -> `k<128, 0, 8, 0>`."""
-    base = kernel.replace("<unnamed>::", "").replace("(anonymous namespace)::", "").split("(")[0]
+    base = re.sub(r"<?unnamed>::|\(anonymous namespace\)::", "", kernel).split("(")[0]
     base = re.sub(r"^void\s+", "", base)
     head, sep, tmpl = base.partition("<")
     if sep:

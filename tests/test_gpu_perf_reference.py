@@ -19,38 +19,99 @@ CONFIGS = [
 ]
 
 
+def _record(result):
+    out = os.environ.get("WFB_PERF_OUT")
+    if out:
+        with open(out, "a") as f:
+            f.write(json.dumps(result) + "\n")
+    print(result)
+
+
+def _best_ms(r, params, reps=3):
+    r.render(params)  # warm-up
+    best = None
+    for _ in range(reps):
+        st = load_engine().RenderStats()
+        img = r.render(params, st)
+        best = st.render_ms if best is None else min(best, st.render_ms)
+    return best, img
+
+
 @pytest.mark.parametrize("scene,w,h,spp", CONFIGS)
 def test_faster_than_reference_megakernel_with_equal_image(ref, scene, w, h, spp):
     wfb = load_engine()
     sc = wfb.Scene.generate(scene, w, h, 1234, 16)
     arrays = sc.export()
     params = wfb.RenderParams(spp=spp, seed=1234, max_depth=8)
-    r = wfb.GpuRenderer(sc, wfb.MEGAKERNEL)
-    r.render(params)  # warm-up
-    mine_ms = []
-    for _ in range(3):
-        st = wfb.RenderStats()
-        img = r.render(params, st)
-        mine_ms.append(st.render_ms)
+    tune = wfb.autotune(sc, w, h, probe_spp=2, max_depth=8, try_wavefront=True)
+    mk = wfb.GpuRenderer(sc, wfb.MEGAKERNEL)
+    mk.apply_tuning(tune)
+    mk_ms, img = _best_ms(mk, params)
+    wf = wfb.GpuRenderer(sc, wfb.WAVEFRONT)
+    wf.apply_tuning(tune)
+    wf_ms, wimg = _best_ms(wf, params)
+    assert np.array_equal(wimg.rgb.view(np.uint32), img.rgb.view(np.uint32))
     t0 = time.perf_counter()
     rrgb, rvar, rst = ref.ref_render_gpu(arrays, 0, spp, 1234, 8)
     ref_wall = time.perf_counter() - t0
     assert np.array_equal(img.rgb.view(np.uint32), rrgb.view(np.uint32)), "image differs from the reference megakernel"
     samples = w * h * spp
     result = {
-        "scene": scene, "size": f"{w}x{h}", "spp": spp, "samples": samples,
-        "engine_megakernel_ms": min(mine_ms), "engine_megakernel_msamples_s": samples / min(mine_ms) / 1e3,
+        "scene": scene, "size": f"{w}x{h}", "spp": spp, "samples": samples, "tuning": tune.as_dict(),
+        "engine_megakernel_ms": mk_ms, "engine_megakernel_msamples_s": samples / mk_ms / 1e3,
+        "engine_wavefront_ms": wf_ms, "engine_wavefront_msamples_s": samples / wf_ms / 1e3,
         "reference_megakernel_ms": rst["render_ms"], "reference_megakernel_msamples_s": samples / rst["render_ms"] / 1e3,
         "reference_megakernel_wall_s": ref_wall,
     }
-    if scene != "heightfield":
+    if scene != "heightfield":  # the reference wavefront needs ~0.5 GB per 1M paths; kept to configs 1-2
         wrgb, _, wst = ref.ref_render_gpu(arrays, 1, spp, 1234, 8)
         assert np.array_equal(wrgb.view(np.uint32), rrgb.view(np.uint32))
         result["reference_wavefront_ms"] = wst["render_ms"]
         result["reference_wavefront_msamples_s"] = samples / wst["render_ms"] / 1e3
-    out = os.environ.get("WFB_PERF_OUT")
-    if out:
-        with open(out, "a") as f:
-            f.write(json.dumps(result) + "\n")
-    print(result)
+    _record(result)
     assert result["engine_megakernel_msamples_s"] > result["reference_megakernel_msamples_s"]
+
+
+def test_mixed_job_stream_against_reference_plain_megakernel(ref):
+    """The 64-job mix (scenes of configs 1-3, uneven resolution / spp / depth / camera): the batched
+    engine (one persistent launch, graph replay), the engine one job per launch, and the reference's
+    plain megakernel one job per launch (one launch per sample) -- device time for all three, and
+    every job's image bit-equal to the reference's render of the same job."""
+    wfb = load_engine()
+    scenes = {name: wfb.Scene.generate(name, 64, 64, 1234, 16) for name in wfb.MIX_SCENES}
+    base = {name: sc.export() for name, sc in scenes.items()}
+    mix = wfb.job_mix(64, 1234)
+    jobs = [(m, scenes[m["scene"]], wfb.mix_job_desc(m, scenes[m["scene"]])) for m in mix]
+    samples = sum(j.width * j.height * j.spp for _, _, j in jobs)
+    b = wfb.Batch(max_jobs=64, use_graph=True)
+    for _, s, j in jobs:
+        b.add(s, j)
+    b.run()
+    batched_ms = min(b.run().render_ms for _ in range(2))
+    plain_ms = 0.0
+    ref_ms = 0.0
+    for k, (m, s, j) in enumerate(jobs):
+        r = wfb.GpuRenderer(s, wfb.MEGAKERNEL)
+        r.set_camera(j.cam_position, j.cam_look_at, j.cam_up, j.cam_vfov_deg, j.width, j.height)
+        st = wfb.RenderStats()
+        solo = r.render(wfb.RenderParams(spp=j.spp, seed=j.seed, max_depth=j.max_depth), st)
+        plain_ms += st.render_ms
+        r.close()
+        arrays = dict(base[m["scene"]], cam_position=list(j.cam_position), cam_look_at=list(j.cam_look_at),
+                      cam_up=list(j.cam_up), cam_vfov_deg=j.cam_vfov_deg, width=j.width, height=j.height)
+        rrgb, _, rst = ref.ref_render_gpu(arrays, 0, j.spp, j.seed, j.max_depth)
+        ref_ms += rst["render_ms"]
+        batch_rgb = b.download(k).rgb
+        assert np.array_equal(batch_rgb.view(np.uint32), rrgb.view(np.uint32)), f"job {k} differs from the reference"
+        assert np.array_equal(solo.rgb.view(np.uint32), rrgb.view(np.uint32))
+    b.close()
+    result = {
+        "workload": "64-job mix (seed 1234)", "samples": samples,
+        "engine_batched_ms": batched_ms, "engine_batched_msamples_s": samples / batched_ms / 1e3,
+        "engine_one_job_per_launch_ms": plain_ms, "engine_one_job_per_launch_msamples_s": samples / plain_ms / 1e3,
+        "reference_megakernel_ms": ref_ms, "reference_megakernel_msamples_s": samples / ref_ms / 1e3,
+        "batched_vs_reference_megakernel": ref_ms / batched_ms,
+        "batched_vs_engine_one_job_per_launch": plain_ms / batched_ms,
+    }
+    _record(result)
+    assert batched_ms < plain_ms < ref_ms
