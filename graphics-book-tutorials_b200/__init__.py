@@ -102,7 +102,8 @@ STAGE_NAMES = ("extend", "classify", "shade_lambert", "shade_metal", "shade_diel
 
 class _CTuneResult(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("block", ctypes.c_int), ("occupancy", ctypes.c_int),
-                ("min_active", ctypes.c_int), ("paths_in_flight", ctypes.c_int), ("wf_min_active", ctypes.c_int),
+                ("min_active", ctypes.c_int), ("leaf_batch", ctypes.c_int), ("paths_in_flight", ctypes.c_int),
+                ("wf_min_active", ctypes.c_int),
                 ("msamples_s", ctypes.c_double),
                 ("megakernel_msamples_s", ctypes.c_double), ("wavefront_msamples_s", ctypes.c_double),
                 ("candidates", ctypes.c_int)]
@@ -198,7 +199,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_renderer_download_sums": (i32, [vp, vp, vp, vp]),
         "wfb_renderer_render": (i32, [vp, ctypes.POINTER(_CRenderParams), ctypes.POINTER(_CRenderStats), vp, vp]),
         "wfb_renderer_device_bytes": (u64, [vp]),
-        "wfb_renderer_configure": (i32, [vp, i32, i32, i32, i32, i32, i32]),
+        "wfb_renderer_configure": (i32, [vp, i32, i32, i32, i32, i32, i32, i32]),
         "wfb_renderer_width": (i32, [vp]),
         "wfb_renderer_height": (i32, [vp]),
         "wfb_renderer_destroy": (i32, [vp]),
@@ -392,10 +393,10 @@ class GpuRenderer:
         return int(load_library().wfb_renderer_device_bytes(self._h))
 
     def configure(self, block: int = -1, blocks_per_sm: int = -1, min_active: int = -1, split_chunks: int = -1,
-                  paths_in_flight: int = -1, occupancy: int = -1) -> None:
+                  paths_in_flight: int = -1, occupancy: int = -1, leaf_batch: int = -1) -> None:
         """Launch knobs (-1 keeps the current setting); see wfb_renderer_configure."""
         _check(load_library().wfb_renderer_configure(self._h, block, blocks_per_sm, min_active, split_chunks,
-                                                      paths_in_flight, occupancy))
+                                                      paths_in_flight, occupancy, leaf_batch))
 
     def apply_tuning(self, tuning: "TuneResult") -> None:
         """Applies the knobs of an autotune result that belong to this renderer's arm."""
@@ -420,6 +421,7 @@ class TuneResult:
     block: int
     occupancy: int
     min_active: int
+    leaf_batch: int
     paths_in_flight: int
     wf_min_active: int
     msamples_s: float
@@ -430,7 +432,8 @@ class TuneResult:
 
     def as_dict(self) -> dict:
         return {"arm": "megakernel" if self.mode == MEGAKERNEL else "wavefront",
-                "megakernel": {"block": self.block, "occupancy": self.occupancy, "min_active": self.min_active},
+                "megakernel": {"block": self.block, "occupancy": self.occupancy, "min_active": self.min_active,
+                               "leaf_batch": self.leaf_batch},
                 "wavefront": {"paths_in_flight": self.paths_in_flight, "min_active": self.wf_min_active},
                 "msamples_s": round(self.msamples_s, 2),
                 "megakernel_msamples_s": round(self.megakernel_msamples_s, 2),
@@ -444,7 +447,8 @@ def autotune(scene: Scene, width: int, height: int, probe_spp: int = 2, max_dept
     c = _CTuneResult()
     _check(load_library().wfb_autotune(scene.handle, int(width), int(height), int(probe_spp), int(max_depth),
                                        1 if try_wavefront else 0, ctypes.byref(c)))
-    return TuneResult(c.mode, c.block, c.occupancy, c.min_active, c.paths_in_flight, c.wf_min_active, c.msamples_s,
+    return TuneResult(c.mode, c.block, c.occupancy, c.min_active, c.leaf_batch, c.paths_in_flight, c.wf_min_active,
+                      c.msamples_s,
                       c.megakernel_msamples_s, c.wavefront_msamples_s, c.candidates, c)
 
 

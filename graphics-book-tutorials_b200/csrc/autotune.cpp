@@ -6,8 +6,9 @@
 // renders the same film bits (launch knobs never change the arithmetic), so tuning is purely a
 // speed decision. Results are cached per (scene hash, width, height, probe_spp, max_depth).
 // The result holds the best knobs of each arm, so a renderer of either arm can apply it.
-//   megakernel: (block, occupancy target) in {(128,8), (128,6), (128,0), (64,0), (256,0)} x
-//               min_active in {8, 16, 20, 24, 28}
+//   megakernel: stage 1, (block, occupancy target) in {(128,8), (128,6), (128,0), (64,0), (256,0)}
+//               x min_active in {8, 16, 24} at leaf_batch 8; stage 2, the stage-1 winner with
+//               leaf_batch in {4, 12, 16, 32}
 //   wavefront:  paths in flight in {512K, 1M, 2M} x min_active {16, 24}; its queues are sized to
 //               the pool, so they never drop a path.
 #include <algorithm>
@@ -58,10 +59,11 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
         Renderer r(scene, wf::GpuMode::Megakernel);
         r.set_camera(cam, width, height);
         const int shapes[][2] = {{128, 8}, {128, 6}, {128, 0}, {64, 0}, {256, 0}};
-        const int actives[] = {8, 16, 20, 24, 28};
+        const int actives[] = {8, 16, 24};
+        best.leaf_batch = 8;
         for (const auto& sh : shapes)
             for (int ma : actives) {
-                r.configure(sh[0], 0, ma, 0, -1, sh[1]);
+                r.configure(sh[0], 0, ma, 0, -1, sh[1], best.leaf_batch);
                 const double ms = measure(r, p);
                 best.candidates++;
                 if (ms < mk_ms) {
@@ -71,6 +73,16 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
                     best.min_active = ma;
                 }
             }
+        const int batches[] = {4, 12, 16, 32};
+        for (int lb : batches) {
+            r.configure(best.block, 0, best.min_active, 0, -1, best.occupancy, lb);
+            const double ms = measure(r, p);
+            best.candidates++;
+            if (ms < mk_ms) {
+                mk_ms = ms;
+                best.leaf_batch = lb;
+            }
+        }
     }
     if (try_wavefront) {
         const int pools[] = {1 << 19, 1 << 20, 1 << 21};
@@ -101,7 +113,7 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
 void apply_tuning(Renderer& r, const TuneResult& t) {
     if (r.mode() == wf::GpuMode::Megakernel)
         r.configure(t.block > 0 ? t.block : -1, -1, t.min_active > 0 ? t.min_active : -1, -1, -1,
-                    t.occupancy >= 0 ? t.occupancy : -1);
+                    t.occupancy >= 0 ? t.occupancy : -1, t.leaf_batch > 0 ? t.leaf_batch : -1);
     else
         r.configure(-1, -1, t.wf_min_active > 0 ? t.wf_min_active : -1, -1,
                     t.paths_in_flight > 0 ? t.paths_in_flight : -1, -1);

@@ -370,14 +370,15 @@ int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render
 uint64_t wfb_renderer_device_bytes(wfb_renderer_t r) { return r ? r->r->device_bytes() : 0; }
 
 int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int min_active, int split_chunks,
-                           int paths_in_flight, int occupancy) {
+                           int paths_in_flight, int occupancy, int leaf_batch) {
     return guarded([&] {
         need(r != nullptr, "null renderer");
         need(block <= 0 || block == 64 || block == 128 || block == 256, "block must be 64, 128 or 256");
         need(min_active <= 32, "min_active must be in 1..32");
         need(occupancy < 0 || occupancy == 0 || ((occupancy == 6 || occupancy == 8) && (block <= 0 || block == 128)),
              "occupancy target must be 0, 6 or 8 (block 128)");
-        r->r->configure(block, blocks_per_sm, min_active, split_chunks, paths_in_flight, occupancy);
+        need(leaf_batch <= 32, "leaf_batch must be in 1..32");
+        r->r->configure(block, blocks_per_sm, min_active, split_chunks, paths_in_flight, occupancy, leaf_batch);
     });
 }
 int wfb_renderer_width(wfb_renderer_t r) { return r ? r->r->width() : 0; }
@@ -399,6 +400,7 @@ int wfb_autotune(wfb_scene_t scene, int width, int height, int probe_spp, int ma
         out->block = t.block;
         out->occupancy = t.occupancy;
         out->min_active = t.min_active;
+        out->leaf_batch = t.leaf_batch;
         out->paths_in_flight = t.paths_in_flight;
         out->wf_min_active = t.wf_min_active;
         out->msamples_s = t.msamples_s;
@@ -416,6 +418,7 @@ int wfb_renderer_apply_tuning(wfb_renderer_t r, const wfb_tune_result* t) {
         tr.block = t->block;
         tr.occupancy = t->occupancy;
         tr.min_active = t->min_active;
+        tr.leaf_batch = t->leaf_batch;
         tr.paths_in_flight = t->paths_in_flight;
         tr.wf_min_active = t->wf_min_active;
         wfb::apply_tuning(*r->r, tr);

@@ -119,62 +119,6 @@ WF_HD wf::LightGeom load_light(const DevScene& s, int idx) {
 }
 
 #if defined(__CUDACC__)
-// Stackless preorder skip-link traversal over the packed nodes: the same visiting order, the
-// same box and primitive arithmetic and the same strictly-nearer replacement rule as
-// wf::intersect (WVM/include/wf/bvh.hpp:91-116), so hit ids, t, u and v are bit-identical.
-// Returns true on a hit. `tests` (optional) accumulates node visits for instrumentation.
-__device__ __forceinline__ bool intersect_dev(const DevScene& s, wf::Ray r, wf::HitRecord* h,
-                                              bool anyhit) {
-    h->t = r.tmax;
-    h->prim = -1;
-    h->u = 0.0f;
-    h->v = 0.0f;
-    const wf::Vec3 inv_d{1.0f / r.d.x, 1.0f / r.d.y, 1.0f / r.d.z};
-    int n = 0;
-    while (n >= 0 && n < s.n_nodes) {
-        const float4 a = __ldg(&s.nodes[2 * n]);
-        const float4 b = __ldg(&s.nodes[2 * n + 1]);
-        const int skip = __float_as_int(a.w);
-        if (!wf::hit_box(wf::Vec3{a.x, a.y, a.z}, wf::Vec3{b.x, b.y, b.z}, r.o, inv_d, r.tmin,
-                         r.tmax)) {
-            n = skip;
-            continue;
-        }
-        const int leaf = __float_as_int(b.w);
-        if (leaf < 0) {
-            n = n + 1;
-            continue;
-        }
-        const int start = leaf >> kLeafCountBits;
-        const int count = leaf & kLeafCountMask;
-        const float4* rec = s.prims + 3 * start;
-        for (int i = 0; i < count; ++i, rec += 3) {
-            const float4 q0 = __ldg(rec);
-            const float4 q1 = __ldg(rec + 1);
-            const int p = __float_as_int(q0.w);
-            float t, u = 0.0f, v = 0.0f;
-            bool hit;
-            if (p < s.n_spheres) {
-                hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
-            } else {
-                const float4 q2 = __ldg(rec + 2);
-                hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
-                                            wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
-            }
-            if (hit) {
-                r.tmax = t;
-                h->t = t;
-                h->prim = p;
-                h->u = u;
-                h->v = v;
-                if (anyhit) return true;
-            }
-        }
-        n = skip;
-    }
-    return h->prim >= 0;
-}
-
 // Slab test of wf::hit_box without the two early exits: t0 only grows and t1 only shrinks
 // (compare-and-select updates that keep the reference's NaN behaviour), so once t0 > t1 the final
 // t0 <= t1 is false as well -- the result is identical, with fewer branches.
@@ -208,22 +152,27 @@ struct TravRay {
     wf::Vec3 d, inv_d;
 };
 
-// One step of the stackless skip-link traversal, resumable between calls: the whole state is the
-// next node index `node` (-1 when done) and the best hit `h` (h.t is the current tmax). Visiting
-// order, box and primitive arithmetic and the strictly-nearer rule are intersect_dev's, so running
-// steps until node < 0 gives bit-identical hits. `anyhit` ends the query at the first hit.
-__device__ __forceinline__ void traversal_step(const float4* __restrict__ nodes, const float4* __restrict__ prims,
-                                               int n_nodes, int n_spheres, const wf::Vec3& o, const TravRay& ray,
-                                               bool anyhit, int& node, wf::HitRecord& h, unsigned& n_prim_tests) {
+// Resumable stackless skip-link traversal over the packed nodes, split into box steps and
+// primitive steps. A ray's whole traversal state is its next node (`node`, -1 when none is left),
+// its pending leaf (`pend`) and its best hit (`h`; h.t is the current tmax).
+//
+// A box step tests the lane's next node; at a leaf whose box the ray enters it records the leaf as
+// pending (`pend` = first record * 16 + count, the node's own leaf encoding; 0 = none) and moves
+// `node` past the leaf (to its skip link). A primitive step tests the next primitive of the pending
+// leaf (pend += 15: next record, one fewer left). Taken one after another until node < 0 and
+// pend == 0, the steps visit nodes and primitives in wf::intersect's order (preorder, skip link on
+// a miss and after a leaf, every primitive of a leaf in leaf order against tmax = the nearest hit
+// so far, a hit replacing the best only when strictly nearer; WVM/include/wf/bvh.hpp:91-116) with
+// its box and primitive arithmetic, so hit ids, t, u and v are bit-identical; `anyhit` ends the
+// query at the first hit. Splitting the steps lets a warp group them: rounds of box steps, and
+// rounds of primitive steps once enough lanes hold a pending leaf, instead of every box round
+// waiting while the one or two lanes that reached a leaf test its primitives one after another.
+__device__ __forceinline__ void box_step(const float4* __restrict__ nodes, int n_nodes, const wf::Vec3& o,
+                                         const TravRay& ray, float tmax, int& node, int& pend) {
     const float4 na = __ldg(&nodes[2 * node]);
     const float4 nb = __ldg(&nodes[2 * node + 1]);
     const int skip = __float_as_int(na.w);
-    wf::Ray r;
-    r.o = o;
-    r.d = ray.d;
-    r.tmin = wf::kRayEps;
-    r.tmax = h.t;
-    if (!hit_box_nobranch(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, r.o, ray.inv_d, r.tmin, r.tmax)) {
+    if (!hit_box_nobranch(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, o, ray.inv_d, wf::kRayEps, tmax)) {
         node = skip;
     } else {
         const int leaf = __float_as_int(nb.w);
@@ -231,37 +180,44 @@ __device__ __forceinline__ void traversal_step(const float4* __restrict__ nodes,
             node = node + 1;
         } else {
             node = skip;
-            const int count = leaf & kLeafCountMask;
-            const float4* rec = prims + 3 * (leaf >> kLeafCountBits);
-            for (int i = 0; i < count; ++i, rec += 3) {
-                const float4 q0 = __ldg(rec);
-                const float4 q1 = __ldg(rec + 1);
-                const int p = __float_as_int(q0.w);
-                float t, u = 0.0f, v = 0.0f;
-                bool hit;
-                ++n_prim_tests;
-                if (p < n_spheres) {
-                    hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
-                } else {
-                    const float4 q2 = __ldg(rec + 2);
-                    hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
-                                                wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
-                }
-                if (hit) {
-                    r.tmax = t;
-                    h.t = t;
-                    h.prim = p;
-                    h.u = u;
-                    h.v = v;
-                    if (anyhit) {
-                        node = -1;
-                        return;
-                    }
-                }
-            }
+            pend = leaf;
         }
     }
     if (node >= n_nodes) node = -1;
+}
+
+__device__ __forceinline__ void prim_step(const float4* __restrict__ prims, int n_spheres, const wf::Vec3& o,
+                                          const TravRay& ray, bool anyhit, int& node, int& pend, wf::HitRecord& h) {
+    const float4* rec = prims + 3 * (pend >> kLeafCountBits);
+    const float4 q0 = __ldg(rec);
+    const float4 q1 = __ldg(rec + 1);
+    const int p = __float_as_int(q0.w);
+    wf::Ray r;
+    r.o = o;
+    r.d = ray.d;
+    r.tmin = wf::kRayEps;
+    r.tmax = h.t;
+    float t, u = 0.0f, v = 0.0f;
+    bool hit;
+    if (p < n_spheres) {
+        hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
+    } else {
+        const float4 q2 = __ldg(rec + 2);
+        hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
+                                    wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
+    }
+    pend += (1 << kLeafCountBits) - 1;
+    if ((pend & kLeafCountMask) == 0) pend = 0;
+    if (hit) {
+        h.t = t;
+        h.prim = p;
+        h.u = u;
+        h.v = v;
+        if (anyhit) {
+            node = -1;
+            pend = 0;
+        }
+    }
 }
 
 // intersect() prologue (WVM/include/wf/bvh.hpp:92-94): the ray's traversal state before step 0.

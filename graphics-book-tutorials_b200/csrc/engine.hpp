@@ -55,6 +55,7 @@ struct MegakernelConfig {
     int min_active = 24;    // traverse on while at least this many lanes of a warp traverse
     int split_chunks = 0;   // work units per pixel; 0: chosen from pixels vs resident lanes
     int occupancy = 8;      // block 128 only: 6 or 8 caps registers for that many CTAs per SM (0: none)
+    int leaf_batch = 8;     // a warp tests primitives once this many lanes hold a pending leaf
 };
 // Resident threads of the persistent megakernel for this configuration.
 int megakernel_resident_threads(const MegakernelConfig& cfg);
@@ -104,6 +105,7 @@ void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
 struct WavefrontConfig {
     int paths_in_flight = 0;  // path-pool slots; 0: 1M (capped at 64 x pixels)
     int min_active = 20;      // traverse on while at least this many lanes of a warp traverse
+    int leaf_batch = 8;       // a warp tests primitives once this many lanes hold a pending leaf
 };
 
 // ---- GPU renderer (renderer.cu): one scene, one camera, one film ----
@@ -135,7 +137,7 @@ public:
     const MegakernelConfig& megakernel_config() const { return mk_cfg_; }
     // Values < 0 keep the current setting (block and min_active also keep on 0).
     void configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight,
-                   int occupancy);
+                   int occupancy, int leaf_batch = -1);
 
 private:
     void alloc_film();

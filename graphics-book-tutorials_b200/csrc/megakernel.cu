@@ -13,8 +13,12 @@
 //    and the tail of one job overlaps the others. Per-job pixel ids stay job-local (the RNG key
 //    uses py * width + px of the job, WVM/include/wf/path_core.hpp:74), so a job renders the same
 //    bits alone and inside any batch.
-//  * Resumable traversal: a ray's traversal state is the next node index plus the best hit
-//    (traversal_step, dev_scene.cuh). A warp keeps stepping all traversing lanes while at least
+//  * Resumable traversal: a ray's traversal state is the next node index, a pending leaf and the
+//    best hit (box_step / prim_step, dev_scene.cuh). A warp runs rounds of box steps (lanes without
+//    a pending leaf test their next node) and rounds of primitive steps (lanes with a pending leaf
+//    test its next primitive), choosing a primitive round once `leaf_batch` lanes hold a pending
+//    leaf or they outnumber the box lanes, so leaf work is done by many lanes at once instead of
+//    by the one or two lanes that reach a leaf in a given box round. It keeps going while at least
 //    `min_active` lanes traverse; only then does it shade the lanes whose ray finished and give
 //    them their next ray (extension, the pending shadow ray of a Lambertian bounce, or the camera
 //    ray of the next sample) -- the "dynamic ray fetch" of Aila and Laine (HPG 2009) with
@@ -47,6 +51,7 @@ struct MkArgs {
     unsigned int* work;
     int count_rays;
     int min_active;
+    int leaf_batch;
 };
 
 template <bool MULTI>
@@ -74,6 +79,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
     // ---- traversal state of the lane's current ray. Every ray starts at ps.ray.o (the camera,
     // or p + n * eps for both the next extension ray and the shadow ray) with tmin = kRayEps. ----
     int node = -1;
+    int pend = 0;  // pending leaf (box_step / prim_step)
     TravRay ray;
     wf::HitRecord h;
     h.t = 0.f;
@@ -89,34 +95,43 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
         const int nn = MULTI ? jn_nodes : a.job0.s.n_nodes;
         if (shadow_ray) traversal_begin(nn, sh_dir, sh_tmax, &ray, &node, &h);
         else traversal_begin(nn, ps.ray.d, ps.ray.tmax, &ray, &node, &h);
+        pend = 0;
     };
     auto new_path = [&](const DevScene& s, uint32_t seed) {
         ps = wf::init_path(s, pixel % s.width, pixel / s.width, (uint32_t)sample, seed);
     };
 
     for (;;) {
-        // ================= traversal: step all traversing lanes, one node each =================
+        // ================= traversal: rounds of box steps or of primitive steps =================
         for (;;) {
-            const bool trav = node >= 0;
-            const unsigned tmask = __ballot_sync(kFull, trav);
+            const bool in_leaf = pend != 0;
+            const bool at_box = node >= 0 && !in_leaf;
+            const unsigned pmask = __ballot_sync(kFull, in_leaf);
+            const unsigned bmask = __ballot_sync(kFull, at_box);
+            const unsigned tmask = pmask | bmask;
             if (tmask == 0) break;
             if (__popc(tmask) < a.min_active) {
                 // few lanes left traversing: stop if some other lane has shading or refill to do
-                const bool waiting = !trav && (pixel >= 0 || !out_of_work);
+                const bool waiting = !(in_leaf || at_box) && (pixel >= 0 || !out_of_work);
                 if (__ballot_sync(kFull, waiting) != 0) break;
             }
-            if (trav) {
+            // primitive round once enough lanes hold a pending leaf (or they outnumber the box lanes)
+            const int np = __popc(pmask);
+            if (np != 0 && (np >= a.leaf_batch || np >= __popc(bmask))) {
+                if (in_leaf) {
+                    if (COUNT) ++n_prims;
+                    if (MULTI) prim_step(jprims, jn_spheres, ps.ray.o, ray, shadow_ray, node, pend, h);
+                    else prim_step(a.job0.s.prims, a.job0.s.n_spheres, ps.ray.o, ray, shadow_ray, node, pend, h);
+                }
+            } else if (at_box) {
                 if (COUNT) ++n_steps;
-                if (MULTI)
-                    traversal_step(jnodes, jprims, jn_nodes, jn_spheres, ps.ray.o, ray, shadow_ray, node, h, n_prims);
-                else
-                    traversal_step(a.job0.s.nodes, a.job0.s.prims, a.job0.s.n_nodes, a.job0.s.n_spheres, ps.ray.o, ray,
-                                   shadow_ray, node, h, n_prims);
+                if (MULTI) box_step(jnodes, jn_nodes, ps.ray.o, ray, h.t, node, pend);
+                else box_step(a.job0.s.nodes, a.job0.s.n_nodes, ps.ray.o, ray, h.t, node, pend);
             }
         }
 
         // ================= shading: lanes whose ray has finished =================
-        if (node < 0 && pixel >= 0) {
+        if (node < 0 && pend == 0 && pixel >= 0) {
             const JobDesc& J = job_at<MULTI>(a, job);
             const DevScene& s = J.s;
             bool path_done = false;
@@ -407,6 +422,7 @@ int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* count
     args.work = work_counter;
     args.count_rays = p.count_rays ? 1 : 0;
     args.min_active = cfg.min_active;
+    args.leaf_batch = cfg.leaf_batch;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
     launch_any<false>(args, args.job0.units, cfg, stream);
     if (args.job0.chunks > 1) {
@@ -426,6 +442,7 @@ void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
     args.work = work_counter;
     args.count_rays = count_rays ? 1 : 0;
     args.min_active = cfg.min_active;
+    args.leaf_batch = cfg.leaf_batch;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
     launch_any<true>(args, 0, cfg, stream);  // full persistent grid: the unit count lives on the device
     int dev = 0, sms = 0;

@@ -152,15 +152,17 @@ void Renderer::download(int spp_done, float* rgb, float* lum_var) {
 void Renderer::download_mean(int spp_done, float* rgb) { download(spp_done, rgb, nullptr); }
 
 void Renderer::configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight,
-                         int occupancy) {
+                         int occupancy, int leaf_batch) {
     if (block > 0) mk_cfg_.block = block;
     if (blocks_per_sm >= 0) mk_cfg_.blocks_per_sm = blocks_per_sm;
     if (min_active > 0) mk_cfg_.min_active = min_active;
     if (split_chunks >= 0) mk_cfg_.split_chunks = split_chunks;
     if (occupancy >= 0) mk_cfg_.occupancy = occupancy;
-    if (mode_ == wf::GpuMode::Wavefront && (paths_in_flight > 0 || min_active > 0)) {
+    if (leaf_batch > 0) mk_cfg_.leaf_batch = leaf_batch;
+    if (mode_ == wf::GpuMode::Wavefront && (paths_in_flight > 0 || min_active > 0 || leaf_batch > 0)) {
         if (paths_in_flight > 0) wf_cfg_.paths_in_flight = paths_in_flight;
         if (min_active > 0) wf_cfg_.min_active = min_active;
+        if (leaf_batch > 0) wf_cfg_.leaf_batch = leaf_batch;
         cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
         wf_.reset();
         wf_ = std::make_unique<Wavefront>(pixels(), wf_cfg_);

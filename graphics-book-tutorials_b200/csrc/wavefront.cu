@@ -90,6 +90,7 @@ struct WfArgs {
     int max_depth;
     uint32_t qcap;  // queue capacity (test hook); capacity otherwise
     int min_active;
+    int leaf_batch;
     int split_shading;  // stage timing: a barrier between material queues
 };
 
@@ -173,6 +174,7 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
     int item = -1;  // list position, -1: none
     uint32_t id = 0;  // slot (extend) or shadow record (shadow) of the current ray
     int node = -1;
+    int pend = 0;  // pending leaf (box_step / prim_step)
     wf::Vec3 o{0.f, 0.f, 0.f};
     TravRay ray;
     wf::HitRecord h;
@@ -180,7 +182,6 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
     h.prim = -1;
     h.u = h.v = 0.f;
     bool exhausted = false;
-    unsigned n_prim_tests = 0;  // (the wavefront reports ray counts only)
     for (;;) {
         // refill lanes without a ray
         const bool need = item < 0 && !exhausted;
@@ -201,22 +202,32 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
                     const float4 d = SHADOW ? P.sh_dir[id] : P.ray_d[id];
                     o = wf::Vec3{oo.x, oo.y, oo.z};
                     traversal_begin(s.n_nodes, wf::Vec3{d.x, d.y, d.z}, d.w, &ray, &node, &h);
+                    pend = 0;
                 } else {
                     exhausted = true;
                 }
             }
         }
         if (__ballot_sync(kFull, item >= 0) == 0) return;
-        // step every traversing lane while enough lanes traverse (or nothing is left to fetch)
+        // rounds of box steps or primitive steps while enough lanes traverse (or nothing is left
+        // to fetch); see box_step / prim_step
         for (;;) {
-            const bool trav = node >= 0;
-            const unsigned tm = __ballot_sync(kFull, trav);
+            const bool in_leaf = pend != 0;
+            const bool at_box = node >= 0 && !in_leaf;
+            const unsigned pm = __ballot_sync(kFull, in_leaf);
+            const unsigned bm = __ballot_sync(kFull, at_box);
+            const unsigned tm = pm | bm;
             if (tm == 0) break;
-            if (__popc(tm) < a.min_active && __ballot_sync(kFull, !trav && !exhausted) != 0) break;
-            if (trav) traversal_step(s.nodes, s.prims, s.n_nodes, s.n_spheres, o, ray, SHADOW, node, h, n_prim_tests);
+            if (__popc(tm) < a.min_active && __ballot_sync(kFull, !(in_leaf || at_box) && !exhausted) != 0) break;
+            const int np = __popc(pm);
+            if (np != 0 && (np >= a.leaf_batch || np >= __popc(bm))) {
+                if (in_leaf) prim_step(s.prims, s.n_spheres, o, ray, SHADOW, node, pend, h);
+            } else if (at_box) {
+                box_step(s.nodes, s.n_nodes, o, ray, h.t, node, pend);
+            }
         }
         // retire finished rays
-        if (item >= 0 && node < 0) {
+        if (item >= 0 && node < 0 && pend == 0) {
             ++*n_rays;
             if (SHADOW) {
                 if (h.prim < 0) {  // unoccluded: L += contrib
@@ -621,6 +632,7 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
     a.max_depth = p.max_depth;
     a.qcap = (p.queue_capacity > 0 && p.queue_capacity < capacity_) ? (uint32_t)p.queue_capacity : (uint32_t)capacity_;
     a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
+    a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = p.stage_timing ? 1 : 0;
     Control* ctl = st.pool.ctl;
     cuda_check(cudaMemsetAsync(ctl, 0, sizeof(Control), stream), "memset control");

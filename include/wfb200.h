@@ -166,9 +166,11 @@ uint64_t wfb_renderer_device_bytes(wfb_renderer_t r);
  * keeps the current setting. Megakernel: block 64/128/256 threads, CTAs per SM (0: all that fit),
  * the minimum number of traversing lanes per warp before shading runs (1..32), work units per
  * pixel (0: automatic), occupancy target (block 128: 0 none, 6 or 8 CTAs per SM by a register
- * cap). Wavefront: paths in flight and min_active. */
+ * cap), and leaf_batch (1..32): a warp runs a round of primitive tests once this many of its
+ * lanes hold a pending leaf (or they outnumber the lanes testing boxes). Wavefront: paths in
+ * flight, min_active and leaf_batch. */
 int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int min_active,
-                           int split_chunks, int paths_in_flight, int occupancy);
+                           int split_chunks, int paths_in_flight, int occupancy, int leaf_batch);
 int wfb_renderer_width(wfb_renderer_t r);
 int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */
@@ -177,11 +179,11 @@ int wfb_renderer_destroy(wfb_renderer_t r);
 /* ---- autotuner (no reference counterpart) ------------------------------------------------------
  * Measures launch configurations of both arms on `scene` (its camera) at width x height for
  * probe_spp samples: the faster arm (mode), the best megakernel block / occupancy target /
- * min_active and the best wavefront paths in flight / min_active (0 when the wavefront was not
- * tried). Cached per scene hash and size. */
+ * min_active / leaf_batch and the best wavefront paths in flight / min_active (0 when the
+ * wavefront was not tried). Cached per scene hash and size. */
 typedef struct {
     int mode;
-    int block, occupancy, min_active;
+    int block, occupancy, min_active, leaf_batch;
     int paths_in_flight, wf_min_active;
     double msamples_s, megakernel_msamples_s, wavefront_msamples_s;
     int candidates;
