@@ -185,7 +185,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_scene_info_get": (i32, [vp, ctypes.POINTER(SceneInfo)]),
         "wfb_scene_export": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
         "wfb_scene_hash": (u64, [vp]),
-        "wfb_scene_rebuild_bvh": (i32, [vp, i32, i32, ctypes.c_float]),
+        "wfb_scene_rebuild_bvh": (i32, [vp, i32, i32, ctypes.c_float, i32]),
         "wfb_scene_validate_bvh": (i32, [vp, ctypes.c_char_p, i32]),
         "wfb_scene_destroy": (i32, [vp]),
         "wfb_scene_device_bytes": (u64, [vp]),
@@ -295,9 +295,10 @@ class Scene:
     def hash(self) -> int:
         return int(load_library().wfb_scene_hash(self._h))
 
-    def rebuild_bvh(self, bins: int = 16, max_leaf: int = 4, traversal_cost: float = 1.0) -> None:
+    def rebuild_bvh(self, bins: int = 16, max_leaf: int = 4, traversal_cost: float = 1.0, threads: int = 0) -> None:
         """Rebuilds the BVH with SAH knobs (before the first upload); see wfb_scene_rebuild_bvh."""
-        _check(load_library().wfb_scene_rebuild_bvh(self._h, int(bins), int(max_leaf), float(traversal_cost)))
+        _check(load_library().wfb_scene_rebuild_bvh(self._h, int(bins), int(max_leaf), float(traversal_cost),
+                                                     int(threads)))
 
     def validate_bvh(self) -> str:
         buf = ctypes.create_string_buffer(256)

@@ -1,4 +1,5 @@
 // extern "C" boundary (include/wfb200.h): status codes instead of exceptions, opaque handles.
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <memory>
@@ -149,7 +150,7 @@ int wfb_device_facts_get(wfb_device_facts* out) {
         size_t free_b = 0, total_b = 0;
         wfb::cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
         std::memset(out, 0, sizeof(*out));
-        std::strncpy(out->name, prop.name, sizeof(out->name) - 1);
+        std::memcpy(out->name, prop.name, std::min(sizeof(out->name) - 1, std::strlen(prop.name)));
         cudaDriverGetVersion(&out->driver_version);
         cudaRuntimeGetVersion(&out->runtime_version);
         out->cc_major = prop.major;
@@ -252,12 +253,12 @@ int wfb_scene_export(wfb_scene_t s, void* spheres, float* vertices, int* triangl
 
 uint64_t wfb_scene_hash(wfb_scene_t s) { return s ? wf::scene_hash(s->host) : 0; }
 
-int wfb_scene_rebuild_bvh(wfb_scene_t s, int bins, int max_leaf, float traversal_cost) {
+int wfb_scene_rebuild_bvh(wfb_scene_t s, int bins, int max_leaf, float traversal_cost, int threads) {
     return guarded([&] {
         need(s != nullptr, "null scene");
         std::lock_guard<std::mutex> lock(s->mu);
         if (s->resident) throw wfb::Error(WFB_ERR_INVALID_ARGUMENT, "scene is already uploaded; rebuild before use");
-        wf::build_bvh_options(s->host, bins, max_leaf, traversal_cost);
+        wf::build_bvh_options(s->host, bins, max_leaf, traversal_cost, threads);
     });
 }
 

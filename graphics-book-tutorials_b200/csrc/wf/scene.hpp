@@ -116,7 +116,8 @@ void build_bvh_bins(Scene& scene, int sah_bins);
 // SAH builder knobs (bins == 8 selects the reference-compatible policy and ignores the others):
 // leaves hold at most max_leaf primitives (1..15); a node of <= max_leaf primitives becomes a
 // leaf unless a split is cheaper with traversal cost `traversal_cost` (intersection cost 1).
-void build_bvh_options(Scene& scene, int sah_bins, int max_leaf, float traversal_cost);
+// Subtrees are built on `threads` threads (0: all cores); the tree does not depend on it.
+void build_bvh_options(Scene& scene, int sah_bins, int max_leaf, float traversal_cost, int threads = 0);
 std::string validate_bvh(const Scene& scene);
 Scene make_scene(const std::string& name, int width, int height);
 Scene load_obj(const std::string& path, int width, int height);

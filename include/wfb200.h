@@ -105,8 +105,9 @@ uint64_t wfb_scene_hash(wfb_scene_t scene);
 /* Rebuilds the BVH of a scene not yet uploaded, with SAH knobs: bins (8 = reference-compatible
  * policy), leaves of at most max_leaf primitives (1..15), traversal_cost relative to one
  * primitive test. Replaces wf::build_bvh (WVM/src/bvh_build.cpp:228-251) for tuning; the tree
- * stays in the preorder skip-link layout. */
-int wfb_scene_rebuild_bvh(wfb_scene_t scene, int bins, int max_leaf, float traversal_cost);
+ * stays in the preorder skip-link layout. Subtrees are built on `threads` host threads (0: all
+ * cores); the tree is the same for every thread count. */
+int wfb_scene_rebuild_bvh(wfb_scene_t scene, int bins, int max_leaf, float traversal_cost, int threads);
 /* Replaces wf::validate_bvh (WVM/src/bvh_build.cpp:253-323): writes "" when valid. */
 int wfb_scene_validate_bvh(wfb_scene_t scene, char* msg, int len);
 /* Releases the caller's reference; device arrays live until the last renderer using them is gone. */

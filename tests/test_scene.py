@@ -91,3 +91,16 @@ def test_invalid_scene_messages(wfb):
         wfb.Scene.from_arrays(dict(bad, vertices=v), finalize_bins=8)
     with pytest.raises(wfb.WfbError, match="no primitives"):
         wfb.Scene.from_arrays(dict(bad, triangles=bad["triangles"][:0]), finalize_bins=8)
+
+
+@pytest.mark.parametrize("name,bins", [("icospheres", 16), ("icospheres", 8), ("cornell36", 16)])
+def test_parallel_bvh_build_is_identical_to_single_threaded(wfb, name, bins):
+    """Subtrees built on many threads stitch into exactly the single-threaded tree."""
+    out = {}
+    for threads in (1, 3, 8):
+        s = wfb.Scene.generate(name, 64, 36, 1234, 16)
+        s.rebuild_bvh(bins=bins, max_leaf=4, traversal_cost=0.5, threads=threads)
+        assert s.validate_bvh() == ""
+        e = s.export()
+        out[threads] = (e["nodes"].tobytes(), e["prim_order"].tobytes(), s.hash())
+    assert out[1] == out[3] == out[8]
