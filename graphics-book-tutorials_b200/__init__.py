@@ -526,10 +526,21 @@ class _CJobDesc(ctypes.Structure):
                 ("max_depth", ctypes.c_int)]
 
 
+class _CLaunchConfig(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("use_graph", ctypes.c_int), ("block", ctypes.c_int),
+                ("occupancy", ctypes.c_int), ("min_active", ctypes.c_int), ("leaf_batch", ctypes.c_int),
+                ("paths_in_flight", ctypes.c_int)]
+
+
+def _launch_config(mode=0, use_graph=True, block=0, occupancy=-1, min_active=0, leaf_batch=0,
+                   paths_in_flight=0) -> _CLaunchConfig:
+    return _CLaunchConfig(int(mode), int(bool(use_graph)), int(block), int(occupancy), int(min_active),
+                          int(leaf_batch), int(paths_in_flight))
+
+
 class _CServerConfig(ctypes.Structure):
     _fields_ = [("budget_bytes", ctypes.c_uint64), ("max_jobs", ctypes.c_int), ("launch_target_ms", ctypes.c_double),
-                ("fixed_slice", ctypes.c_int), ("one_job_per_launch", ctypes.c_int), ("use_graph", ctypes.c_int),
-                ("block", ctypes.c_int), ("min_active", ctypes.c_int)]
+                ("fixed_slice", ctypes.c_int), ("one_job_per_launch", ctypes.c_int), ("launch", _CLaunchConfig)]
 
 
 class _CServerStats(ctypes.Structure):
@@ -568,7 +579,7 @@ def _bind_batch_server(lib):
     vp, i32, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64
     jd = ctypes.POINTER(_CJobDesc)
     sig = {
-        "wfb_batch_create": (i32, [i32, i32, i32, i32, ctypes.POINTER(vp)]),
+        "wfb_batch_create": (i32, [i32, ctypes.POINTER(_CLaunchConfig), ctypes.POINTER(vp)]),
         "wfb_batch_add": (i32, [vp, vp, jd, ctypes.POINTER(i32)]),
         "wfb_batch_clear": (i32, [vp]),
         "wfb_batch_run": (i32, [vp, i32, ctypes.POINTER(_CRenderStats)]),
@@ -595,10 +606,14 @@ def _bind_batch_server(lib):
 class Batch:
     """Many jobs in one persistent launch (wfb_batch_*); every job's film equals its solo render."""
 
-    def __init__(self, max_jobs: int = 64, use_graph: bool = True, block: int = 0, min_active: int = 0):
+    def __init__(self, max_jobs: int = 64, use_graph: bool = True, block: int = 0, min_active: int = 0,
+                 mode: int = MEGAKERNEL, occupancy: int = -1, leaf_batch: int = 0, paths_in_flight: int = 0):
+        """mode MEGAKERNEL (graph replay when use_graph) or WAVEFRONT (pool of paths_in_flight slots);
+        knobs <= 0 (occupancy < 0) keep the defaults."""
         lib = _bind_batch_server(load_library())
         h = ctypes.c_void_p()
-        _check(lib.wfb_batch_create(int(max_jobs), int(bool(use_graph)), int(block), int(min_active), ctypes.byref(h)))
+        cfg = _launch_config(mode, use_graph, block, occupancy, min_active, leaf_batch, paths_in_flight)
+        _check(lib.wfb_batch_create(int(max_jobs), ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
         self._jobs = []
         self._scenes = []
@@ -652,10 +667,12 @@ class Server:
 
     def __init__(self, budget_bytes: int = 0, max_jobs: int = 0, launch_target_ms: float = 0.0,
                  fixed_slice: int = 0, one_job_per_launch: bool = False, use_graph: bool = True, block: int = 0,
-                 min_active: int = 0):
+                 min_active: int = 0, mode: int = MEGAKERNEL, occupancy: int = -1, leaf_batch: int = 0,
+                 paths_in_flight: int = 0):
         lib = _bind_batch_server(load_library())
         cfg = _CServerConfig(int(budget_bytes), int(max_jobs), float(launch_target_ms), int(fixed_slice),
-                             int(bool(one_job_per_launch)), int(bool(use_graph)), int(block), int(min_active))
+                             int(bool(one_job_per_launch)),
+                             _launch_config(mode, use_graph, block, occupancy, min_active, leaf_batch, paths_in_flight))
         h = ctypes.c_void_p()
         _check(lib.wfb_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -1,5 +1,6 @@
 // Batched rendering: many jobs of uneven size (scene, camera, resolution, spp, depth, seed) in one
-// persistent megakernel launch, replayed through a CUDA graph captured once per launch shape.
+// persistent launch of either arm: the megakernel (replayed through a CUDA graph captured once per
+// launch shape) or the wavefront (paths of all jobs in one pool; each slot carries its job id).
 //
 // Every job renders exactly the bits it renders alone: pixel ids and RNG keys are job-local,
 // and a pixel's samples are added in ascending order whatever the batch (see megakernel.cu).
@@ -37,10 +38,14 @@ void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var
 }
 
 // ---------------------------------------------------------------------------------------------
-BatchLauncher::BatchLauncher(int max_jobs, const MegakernelConfig& cfg, bool use_graph)
-    : max_jobs_(max_jobs), cfg_(cfg), use_graph_(use_graph) {
+BatchLauncher::BatchLauncher(int max_jobs, const LaunchConfig& cfg) : max_jobs_(max_jobs), cfg_(cfg) {
     if (max_jobs <= 0 || max_jobs > 65535) throw Error(WFB_ERR_INVALID_ARGUMENT, "max_jobs must be in 1..65535");
-    resident_lanes_ = megakernel_resident_threads(cfg_);
+    if (cfg_.mode == wf::GpuMode::Wavefront) {
+        wf_ = std::make_unique<WavefrontEngine>(1 << 24, cfg_.wf);  // pool sized by paths_in_flight alone
+        resident_lanes_ = wf_->capacity();
+    } else {
+        resident_lanes_ = megakernel_resident_threads(cfg_.mk);
+    }
     const size_t table = sizeof(BatchHeader) + (size_t)max_jobs * sizeof(JobDesc);
     const size_t bytes = table + 256 + sizeof(DevCounters) + 256;
     cuda_check(cudaMalloc(&arena_, bytes), "cudaMalloc batch table");
@@ -100,8 +105,15 @@ void BatchLauncher::launch(const std::vector<JobSpec>& jobs, const std::vector<J
                                cudaMemcpyHostToDevice, stream),
                "upload job table");
     cuda_check(cudaMemsetAsync(d_counters_, 0, sizeof(DevCounters), stream), "zero counters");
-    if (!use_graph_) {
-        launch_megakernel_batch(d_jobs_, d_hdr_, max_jobs_, d_counters_, d_work_, count_rays, cfg_, stream);
+    if (wf_) {
+        last_launches_ = wf_->run_batch(d_jobs_, d_hdr_, d_counters_, count_rays, stream);
+        launch_film_commit_jobs(d_jobs_, d_hdr_, max_jobs_, stream);
+        ++last_launches_;
+        return;
+    }
+    last_launches_ = 2;  // persistent megakernel + film commits
+    if (!cfg_.use_graph) {
+        launch_megakernel_batch(d_jobs_, d_hdr_, max_jobs_, d_counters_, d_work_, count_rays, cfg_.mk, stream);
         return;
     }
     if (graph_exec_ && count_rays_in_graph_ != count_rays) {
@@ -112,7 +124,7 @@ void BatchLauncher::launch(const std::vector<JobSpec>& jobs, const std::vector<J
         cudaGraph_t graph = nullptr;
         cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
         try {
-            launch_megakernel_batch(d_jobs_, d_hdr_, max_jobs_, d_counters_, d_work_, count_rays, cfg_, stream);
+            launch_megakernel_batch(d_jobs_, d_hdr_, max_jobs_, d_counters_, d_work_, count_rays, cfg_.mk, stream);
         } catch (...) {
             cudaStreamEndCapture(stream, &graph);
             if (graph) cudaGraphDestroy(graph);
@@ -135,8 +147,7 @@ DevCounters BatchLauncher::counters(cudaStream_t stream) {
 }
 
 // ---------------------------------------------------------------------------------------------
-BatchRenderer::BatchRenderer(int max_jobs, const MegakernelConfig& cfg, bool use_graph)
-    : launcher_(max_jobs, cfg, use_graph) {
+BatchRenderer::BatchRenderer(int max_jobs, const LaunchConfig& cfg) : launcher_(max_jobs, cfg) {
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreate(&ev0_), "cudaEventCreate");
     cuda_check(cudaEventCreate(&ev1_), "cudaEventCreate");

@@ -5,6 +5,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "engine.hpp"
+#include "wavefront.hpp"
 
 namespace wfb {
 
@@ -25,19 +26,22 @@ struct JobBuffers {
     int chunks = 1;
 };
 
-// Launch machinery shared by the batch API and the server: device job table, counters, and one
-// CUDA graph per launch shape (max_jobs, launch configuration), replayed for every batch.
+// Launch machinery shared by the batch API and the server: device job table, counters, and the
+// arm -- the persistent megakernel (one CUDA graph per launch shape, replayed for every batch) or
+// the persistent wavefront over a pool of paths_in_flight slots.
 class BatchLauncher {
 public:
-    BatchLauncher(int max_jobs, const MegakernelConfig& cfg, bool use_graph);
+    BatchLauncher(int max_jobs, const LaunchConfig& cfg);
     ~BatchLauncher();
     BatchLauncher(const BatchLauncher&) = delete;
     BatchLauncher& operator=(const BatchLauncher&) = delete;
 
     int max_jobs() const { return max_jobs_; }
-    const MegakernelConfig& config() const { return cfg_; }
+    const LaunchConfig& config() const { return cfg_; }
     // Work units per pixel for a job of `pixels` pixels and `samples` samples (split small jobs).
     int chunks_for(int pixels, int samples) const;
+    // Kernels launched by the last launch().
+    int last_launches() const { return last_launches_; }
     // Enqueues one launch over `jobs` (their films must hold the sums to add to); jobs are
     // reordered longest-unit-first on the device table only. Returns after enqueueing.
     void launch(const std::vector<JobSpec>& jobs, const std::vector<JobBuffers>& bufs, bool count_rays,
@@ -48,9 +52,10 @@ public:
 
 private:
     int max_jobs_;
-    MegakernelConfig cfg_;
-    bool use_graph_;
-    int resident_lanes_;
+    LaunchConfig cfg_;
+    int resident_lanes_;  // megakernel lanes or wavefront slots working at once
+    int last_launches_ = 0;
+    std::unique_ptr<WavefrontEngine> wf_;
     void* arena_ = nullptr;  // header + job table + counters + work counter
     BatchHeader* d_hdr_ = nullptr;
     JobDesc* d_jobs_ = nullptr;
@@ -64,7 +69,7 @@ private:
 // Synchronous batch API (wfb_batch_*): owns the films of its jobs.
 class BatchRenderer {
 public:
-    BatchRenderer(int max_jobs, const MegakernelConfig& cfg, bool use_graph);
+    BatchRenderer(int max_jobs, const LaunchConfig& cfg);
     ~BatchRenderer();
     int add(const JobSpec& job);  // returns the job id
     void clear();

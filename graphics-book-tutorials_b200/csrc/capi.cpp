@@ -120,6 +120,25 @@ void need(bool ok, const char* msg) {
     if (!ok) throw wfb::Error(WFB_ERR_INVALID_ARGUMENT, msg);
 }
 
+// wfb_launch_config -> LaunchConfig; NULL or values <= 0 (occupancy < 0) keep the defaults.
+wfb::LaunchConfig launch_config(const wfb_launch_config* c) {
+    wfb::LaunchConfig l;
+    if (c == nullptr) return l;
+    need(c->mode == WFB_MODE_MEGAKERNEL || c->mode == WFB_MODE_WAVEFRONT, "mode must be megakernel or wavefront");
+    l.mode = c->mode == WFB_MODE_WAVEFRONT ? wf::GpuMode::Wavefront : wf::GpuMode::Megakernel;
+    l.use_graph = c->use_graph != 0;
+    if (c->block > 0) l.mk.block = c->block;
+    need(l.mk.block == 64 || l.mk.block == 128 || l.mk.block == 256, "block must be 64, 128 or 256");
+    if (c->occupancy >= 0) l.mk.occupancy = c->occupancy;
+    need(l.mk.occupancy == 0 || ((l.mk.occupancy == 6 || l.mk.occupancy == 8) && l.mk.block == 128),
+         "occupancy target must be 0, 6 or 8 (block 128)");
+    need(c->min_active <= 32 && c->leaf_batch <= 32, "min_active and leaf_batch must be in 1..32");
+    if (c->min_active > 0) l.mk.min_active = l.wf.min_active = c->min_active;
+    if (c->leaf_batch > 0) l.mk.leaf_batch = l.wf.leaf_batch = c->leaf_batch;
+    if (c->paths_in_flight > 0) l.wf.paths_in_flight = c->paths_in_flight;
+    return l;
+}
+
 }  // namespace
 
 extern "C" {
@@ -426,16 +445,11 @@ int wfb_renderer_apply_tuning(wfb_renderer_t r, const wfb_tune_result* t) {
     });
 }
 
-int wfb_batch_create(int max_jobs, int use_graph, int block, int min_active, wfb_batch_t* out) {
+int wfb_batch_create(int max_jobs, const wfb_launch_config* cfg, wfb_batch_t* out) {
     return guarded([&] {
         need(out != nullptr, "null argument");
-        wfb::MegakernelConfig cfg;
-        if (block > 0) cfg.block = block;
-        if (min_active > 0) cfg.min_active = min_active;
-        need(cfg.block == 64 || cfg.block == 128 || cfg.block == 256, "block must be 64, 128 or 256");
-        need(cfg.min_active <= 32, "min_active must be in 1..32");
         auto b = std::make_unique<wfb_batch>();
-        b->b = std::make_unique<wfb::BatchRenderer>(max_jobs, cfg, use_graph != 0);
+        b->b = std::make_unique<wfb::BatchRenderer>(max_jobs, launch_config(cfg));
         *out = b.release();
     });
 }
@@ -466,7 +480,7 @@ int wfb_batch_run(wfb_batch_t b, int count_rays, wfb_render_stats* stats) {
         b->b->run(count_rays != 0, &st);
         if (stats) {
             to_c_stats(st, stats);
-            stats->kernel_launches = 2;  // persistent megakernel over the job table + film commit
+            stats->kernel_launches = (uint64_t)b->b->launcher().last_launches();
         }
     });
 }
@@ -499,10 +513,7 @@ int wfb_server_create(const wfb_server_config* c, wfb_server_t* out) {
         if (c->launch_target_ms > 0) cfg.launch_target_ms = c->launch_target_ms;
         cfg.fixed_slice = c->fixed_slice;
         cfg.one_job_per_launch = c->one_job_per_launch != 0;
-        cfg.use_graph = c->use_graph != 0;
-        if (c->block > 0) cfg.cfg.block = c->block;
-        if (c->min_active > 0) cfg.cfg.min_active = c->min_active;
-        need(cfg.cfg.block == 64 || cfg.cfg.block == 128 || cfg.cfg.block == 256, "block must be 64, 128 or 256");
+        cfg.launch = launch_config(&c->launch);
         auto s = std::make_unique<wfb_server>();
         s->s = std::make_unique<wfb::Server>(cfg);
         *out = s.release();

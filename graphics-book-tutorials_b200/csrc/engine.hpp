@@ -94,6 +94,22 @@ struct BatchHeader {
 
 JobDesc make_job(const DevScene& s, const DevFilm& film, float* lbuf, int first_sample, int sample_count,
                  int chunks, uint32_t seed, int max_depth);
+
+#if defined(__CUDACC__)
+// Job owning work unit `u` of a batch: the last job whose first unit is <= u (unit_begin ascends).
+__device__ __forceinline__ int job_of_unit(const JobDesc* jobs, int n_jobs, unsigned u) {
+    int lo = 0, hi = n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].unit_begin <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+#endif
+
+// Split-mode commits of every job of a batch (jobs with chunks > 1), in sample order.
+void launch_film_commit_jobs(const JobDesc* d_jobs, const BatchHeader* d_hdr, int max_jobs, cudaStream_t stream);
 // Persistent megakernel over a device job table (unit_begin must be the running sum of units)
 // followed by the split-mode commits of its jobs; max_jobs bounds the job count of any batch
 // replayed through the same launch. Stream-ordered, no host synchronisation, capturable.
@@ -106,6 +122,14 @@ struct WavefrontConfig {
     int paths_in_flight = 0;  // path-pool slots; 0: 1M (capped at 64 x pixels)
     int min_active = 20;      // traverse on while at least this many lanes of a warp traverse
     int leaf_batch = 8;       // a warp tests primitives once this many lanes hold a pending leaf
+};
+
+// Launch configuration of a batch or a server: the arm and its knobs.
+struct LaunchConfig {
+    wf::GpuMode mode = wf::GpuMode::Megakernel;
+    MegakernelConfig mk{};
+    WavefrontConfig wf{};
+    bool use_graph = true;  // megakernel: replay one captured graph per launch shape
 };
 
 // ---- GPU renderer (renderer.cu): one scene, one camera, one film ----

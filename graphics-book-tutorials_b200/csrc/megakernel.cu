@@ -214,15 +214,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
             if (need) {
                 const unsigned u = base + __popc(need_mask & ((1u << lane) - 1u));
                 if (u < total_units) {
-                    if (MULTI) {  // last job whose first unit is <= u
-                        int lo = 0, hi = n_jobs - 1;
-                        while (lo < hi) {
-                            const int mid = (lo + hi + 1) >> 1;
-                            if (a.jobs[mid].unit_begin <= u) lo = mid;
-                            else hi = mid - 1;
-                        }
-                        job = lo;
-                    }
+                    if (MULTI) job = job_of_unit(a.jobs, n_jobs, u);
                     const JobDesc& J = job_at<MULTI>(a, job);
                     const DevScene& s = J.s;
                     if (MULTI) {
@@ -445,6 +437,10 @@ void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
     args.leaf_batch = cfg.leaf_batch;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
     launch_any<true>(args, 0, cfg, stream);  // full persistent grid: the unit count lives on the device
+    launch_film_commit_jobs(d_jobs, d_hdr, max_jobs, stream);
+}
+
+void launch_film_commit_jobs(const JobDesc* d_jobs, const BatchHeader* d_hdr, int max_jobs, cudaStream_t stream) {
     int dev = 0, sms = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");

@@ -43,7 +43,7 @@ struct Server::Job {
 
 Server::Server(const ServerConfig& cfg) : cfg_(cfg) {
     if (cfg_.one_job_per_launch) cfg_.max_jobs = 1;
-    launcher_ = std::make_unique<BatchLauncher>(cfg_.max_jobs, cfg_.cfg, cfg_.use_graph);
+    launcher_ = std::make_unique<BatchLauncher>(cfg_.max_jobs, cfg_.launch);
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreate(&ev0_), "cudaEventCreate");
     cuda_check(cudaEventCreate(&ev1_), "cudaEventCreate");

@@ -19,8 +19,7 @@ struct ServerConfig {
     double launch_target_ms = 20.0;       // slice size aims at launches of about this length
     int fixed_slice = 0;                  // > 0: samples per job per launch (0: adaptive)
     bool one_job_per_launch = false;      // plain mode: FIFO, whole job, one launch per job
-    bool use_graph = true;
-    MegakernelConfig cfg;
+    LaunchConfig launch;  // arm and knobs of every launch
 };
 
 enum JobState : int { kQueued = 0, kActive = 1, kDone = 2, kCancelled = 3, kFailed = 4 };

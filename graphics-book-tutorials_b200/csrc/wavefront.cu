@@ -76,23 +76,22 @@ struct Pool {
 };
 
 struct WfArgs {
-    DevScene s;
-    DevFilm film;
+    JobDesc job0;             // single render: the one job, in parameter space
+    const JobDesc* jobs;      // batch: device job table (units numbered across jobs)
+    const BatchHeader* hdr;   // batch: job count and total units
     Pool pool;
-    float* lbuf;
     int capacity;
-    int pixels;
-    int first_sample;
-    int sample_count;
-    int chunk;
-    int chunks;
-    uint32_t seed;
-    int max_depth;
     uint32_t qcap;  // queue capacity (test hook); capacity otherwise
     int min_active;
     int leaf_batch;
     int split_shading;  // stage timing: a barrier between material queues
 };
+
+// The job a slot's path belongs to (its unit's .w); a single render has only job0.
+template <bool MULTI>
+__device__ __forceinline__ const JobDesc& job_at(const WfArgs& a, int j) {
+    return MULTI ? a.jobs[j] : a.job0;
+}
 
 __device__ __forceinline__ wf::PathState load_path(const Pool& P, int slot) {
     const float4 o = P.ray_o[slot], d = P.ray_d[slot], t = P.thr[slot], l = P.rad[slot];
@@ -165,11 +164,14 @@ __device__ bool grid_sync(Control* c, unsigned nblocks, int stage, unsigned long
 
 // Resumable closest-hit / any-hit traversal over a list of rays fetched dynamically.
 // Extend: items[i] are slot ids. Shadow: the rays are shadow records 0..n-1 (items unused).
-template <bool SHADOW>
+template <bool SHADOW, bool MULTI>
 __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned n, unsigned* cursor,
                                unsigned long long* n_rays) {
-    const DevScene& s = a.s;
     const Pool& P = a.pool;
+    // BVH of the lane's current ray: a batch reads its job's from the table at fetch time
+    const float4* nodes = a.job0.s.nodes;
+    const float4* prims = a.job0.s.prims;
+    int n_nodes = a.job0.s.n_nodes, n_spheres = a.job0.s.n_spheres;
     const int lane = threadIdx.x & 31;
     int item = -1;  // list position, -1: none
     uint32_t id = 0;  // slot (extend) or shadow record (shadow) of the current ray
@@ -198,10 +200,17 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
                     id = SHADOW ? i : items[i];  // shadow records are numbered by queue position
                     // every ray starts at its path's origin with tmin = kRayEps (see TravRay)
                     const int slot = SHADOW ? __float_as_int(P.sh_c[id].w) : (int)id;
+                    if (MULTI) {
+                        const DevScene& js = a.jobs[P.unit[slot].w].s;
+                        nodes = js.nodes;
+                        prims = js.prims;
+                        n_nodes = js.n_nodes;
+                        n_spheres = js.n_spheres;
+                    }
                     const float4 oo = P.ray_o[slot];
                     const float4 d = SHADOW ? P.sh_dir[id] : P.ray_d[id];
                     o = wf::Vec3{oo.x, oo.y, oo.z};
-                    traversal_begin(s.n_nodes, wf::Vec3{d.x, d.y, d.z}, d.w, &ray, &node, &h);
+                    traversal_begin(n_nodes, wf::Vec3{d.x, d.y, d.z}, d.w, &ray, &node, &h);
                     pend = 0;
                 } else {
                     exhausted = true;
@@ -221,9 +230,9 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
             if (__popc(tm) < a.min_active && __ballot_sync(kFull, !(in_leaf || at_box) && !exhausted) != 0) break;
             const int np = __popc(pm);
             if (np != 0 && (np >= a.leaf_batch || np >= __popc(bm))) {
-                if (in_leaf) prim_step(s.prims, s.n_spheres, o, ray, SHADOW, node, pend, h);
+                if (in_leaf) prim_step(prims, n_spheres, o, ray, SHADOW, node, pend, h);
             } else if (at_box) {
-                box_step(s.nodes, s.n_nodes, o, ray, h.t, node, pend);
+                box_step(nodes, n_nodes, o, ray, h.t, node, pend);
             }
         }
         // retire finished rays
@@ -247,16 +256,16 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
     }
 }
 
+template <bool MULTI>
 __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a) {
-    const DevScene& s = a.s;
     const Pool& P = a.pool;
     Control* c = P.ctl;
     const int lane = threadIdx.x & 31;
     const unsigned nblocks = gridDim.x;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gthreads = gridDim.x * blockDim.x;
-    const bool split = a.chunks > 1;
-    const unsigned total_units = (unsigned)a.pixels * (unsigned)a.chunks;
+    const unsigned total_units = MULTI ? a.hdr->total_units : a.job0.units;
+    const int n_jobs = MULTI ? (int)a.hdr->n_jobs : 1;
     __shared__ uint32_t smem[33];
     __shared__ int s_tile;
     __shared__ uint32_t s_prefix;
@@ -292,10 +301,12 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                 if (!has_path) {
                     u = P.unit[slot];
                     if (u.x >= 0) {
+                        const JobDesc& J = job_at<MULTI>(a, u.w);
+                        const bool split = J.chunks > 1;
                         // commit the finished sample (film_add order, WVM/src/gpu/engine.cuh:25-32)
                         const float4 l = P.rad[slot];
                         if (split) {
-                            float* dst = a.lbuf + 3 * ((size_t)u.x * a.sample_count + (u.y - a.first_sample));
+                            float* dst = J.lbuf + 3 * ((size_t)u.x * J.sample_count + (u.y - J.first_sample));
                             dst[0] = l.x;
                             dst[1] = l.y;
                             dst[2] = l.z;
@@ -313,19 +324,19 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                         }
                         u.y += 1;
                         if (u.y < u.z) {
-                            const int px = u.x % s.width, py = u.x / s.width;
-                            store_path(P, slot, wf::init_path(s, px, py, (uint32_t)u.y, a.seed));
+                            const int px = u.x % J.s.width, py = u.x / J.s.width;
+                            store_path(P, slot, wf::init_path(J.s, px, py, (uint32_t)u.y, J.seed));
                             P.unit[slot] = u;
                             P.alive[slot] = 1u;
                             has_path = true;
                         } else {
                             if (!split) {
                                 const float4 ac = P.acc[slot];
-                                a.film.rgb[3 * u.x] = ac.x;
-                                a.film.rgb[3 * u.x + 1] = ac.y;
-                                a.film.rgb[3 * u.x + 2] = ac.z;
-                                a.film.lum[u.x] = ac.w;
-                                a.film.lum2[u.x] = P.acc2[slot];
+                                J.film.rgb[3 * u.x] = ac.x;
+                                J.film.rgb[3 * u.x + 1] = ac.y;
+                                J.film.rgb[3 * u.x + 2] = ac.z;
+                                J.film.lum[u.x] = ac.w;
+                                J.film.lum2[u.x] = P.acc2[slot];
                             }
                             u.x = -1;
                             P.unit[slot] = u;
@@ -346,17 +357,21 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                 if (need_unit) {
                     const unsigned uid = base + __popc(nm & ((1u << lane) - 1u));
                     if (uid < total_units) {
-                        const int pixel = (int)(uid % (unsigned)a.pixels);
-                        const int ch = (int)(uid / (unsigned)a.pixels);
-                        const int first = a.first_sample + ch * a.chunk;
-                        const int end = min(first + a.chunk, a.first_sample + a.sample_count);
-                        P.unit[slot] = make_int4(pixel, first, end, 0);
-                        if (!split) {
-                            P.acc[slot] = make_float4(a.film.rgb[3 * pixel], a.film.rgb[3 * pixel + 1],
-                                                      a.film.rgb[3 * pixel + 2], a.film.lum[pixel]);
-                            P.acc2[slot] = a.film.lum2[pixel];
+                        // unit -> job, then pixel (local mod P) and chunk (local div P)
+                        const int job = MULTI ? job_of_unit(a.jobs, n_jobs, uid) : 0;
+                        const JobDesc& J = job_at<MULTI>(a, job);
+                        const unsigned local = uid - J.unit_begin;
+                        const int pixel = (int)(local % (unsigned)J.film.pixels);
+                        const int ch = (int)(local / (unsigned)J.film.pixels);
+                        const int first = J.first_sample + ch * J.chunk;
+                        const int end = min(first + J.chunk, J.first_sample + J.sample_count);
+                        P.unit[slot] = make_int4(pixel, first, end, job);
+                        if (J.chunks == 1) {
+                            P.acc[slot] = make_float4(J.film.rgb[3 * pixel], J.film.rgb[3 * pixel + 1],
+                                                      J.film.rgb[3 * pixel + 2], J.film.lum[pixel]);
+                            P.acc2[slot] = J.film.lum2[pixel];
                         }
-                        store_path(P, slot, wf::init_path(s, pixel % s.width, pixel / s.width, (uint32_t)first, a.seed));
+                        store_path(P, slot, wf::init_path(J.s, pixel % J.s.width, pixel / J.s.width, (uint32_t)first, J.seed));
                         P.alive[slot] = 1u;
                         has_path = true;
                     }
@@ -392,7 +407,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
         if (n == 0) break;
 
         // ---------------- E: extension rays ----------------
-        traverse_phase<false>(a, next, n, &c->fetch[0], &n_ext);
+        traverse_phase<false, MULTI>(a, next, n, &c->fetch[0], &n_ext);
         if (!grid_sync(c, nblocks, 0, &t_last)) break;
 
         // ---------------- C: classify, push material queues ----------------
@@ -408,13 +423,14 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                 h.prim = __float_as_int(hv.y);
                 h.u = hv.z;
                 h.v = hv.w;
-                if (!hit_is_valid(s, h)) {
+                const JobDesc& J = job_at<MULTI>(a, MULTI ? P.unit[slot].w : 0);
+                if (!hit_is_valid(J.s, h)) {
                     ++n_invalid;
                     h.prim = -1;  // treated as a miss
                 }
                 wf::PathState ps = load_path(P, slot);
                 wf::Surface f;
-                mat = wf::classify(s, ps, h, a.max_depth, &f);
+                mat = wf::classify(J.s, ps, h, J.max_depth, &f);
                 store_radiance(P, slot, ps);
                 if (mat >= 0) {
                     P.surf_p[slot] = make_float4(f.p.x, f.p.y, f.p.z,
@@ -449,6 +465,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                 wf::Vec3 contrib{0.f, 0.f, 0.f};
                 if (valid) {
                     slot = (int)P.queue[q][i];
+                    const DevScene& s = job_at<MULTI>(a, MULTI ? P.unit[slot].w : 0).s;
                     wf::PathState ps = load_path(P, slot);
                     const float4 sp = P.surf_p[slot], sn = P.surf_n[slot];
                     wf::Surface f;
@@ -487,7 +504,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
         // ---------------- H: shadow rays ----------------
         const unsigned nsh = min(*(volatile unsigned*)&c->qcount[3], a.qcap);
         if (gtid == 0 && nsh > c->high_water[3]) c->high_water[3] = nsh;
-        traverse_phase<true>(a, nullptr, nsh, &c->fetch[1], &n_sh);
+        traverse_phase<true, MULTI>(a, nullptr, nsh, &c->fetch[1], &n_sh);
         if (!grid_sync(c, nblocks, 5, &t_last)) break;
     }
 
@@ -568,7 +585,8 @@ struct WavefrontEngine::State {
     Pool pool{};
     float* lbuf = nullptr;
     size_t lbuf_floats = 0;
-    int grid = 0;
+    int grid = 0;        // co-resident CTAs of the single-render kernel
+    int grid_multi = 0;  // and of the batch kernel
 };
 
 WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixels_(pixels), cfg_(cfg) {
@@ -587,9 +605,12 @@ WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixel
     cuda_check(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cooperative attribute");
     if (!coop) throw Error(WFB_ERR_UNSUPPORTED, "device does not support cooperative launches");
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wavefront_persistent, kWfBlock, 0), "occupancy");
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wavefront_persistent<false>, kWfBlock, 0), "occupancy");
     if (occ < 1) throw Error(WFB_ERR_UNSUPPORTED, "wavefront kernel does not fit on an SM");
     state_->grid = sms * occ;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wavefront_persistent<true>, kWfBlock, 0), "occupancy");
+    if (occ < 1) throw Error(WFB_ERR_UNSUPPORTED, "wavefront batch kernel does not fit on an SM");
+    state_->grid_multi = sms * occ;
 }
 
 WavefrontEngine::~WavefrontEngine() {
@@ -599,25 +620,40 @@ WavefrontEngine::~WavefrontEngine() {
 
 uint64_t WavefrontEngine::bytes() const { return bytes_ + (state_ ? state_->lbuf_floats * sizeof(float) : 0); }
 
+namespace {
+
+// Control reset, pool init, the cooperative launch and the counter fold; returns kernels launched.
+template <bool MULTI>
+int launch_pool(const WfArgs& args, int grid, int capacity, DevCounters* counters, bool count_rays,
+                cudaStream_t stream) {
+    const Pool& pool = args.pool;
+    cuda_check(cudaMemsetAsync(pool.ctl, 0, sizeof(Control), stream), "memset control");
+    cuda_check(cudaMemsetAsync(pool.status, 0, ((size_t)capacity / kWfBlock + 2) * sizeof(unsigned long long), stream),
+               "memset status");
+    wavefront_init<<<(capacity + 255) / 256, 256, 0, stream>>>(pool, capacity);
+    cuda_check(cudaGetLastError(), "wavefront init launch");
+    WfArgs a = args;
+    void* params[] = {&a};
+    cuda_check(cudaLaunchCooperativeKernel((const void*)wavefront_persistent<MULTI>, dim3(grid), dim3(kWfBlock), params,
+                                           0, stream),
+               "wavefront cooperative launch");
+    wavefront_fold<<<1, 1, 0, stream>>>(pool.ctl, counters, count_rays ? 1 : 0);
+    cuda_check(cudaGetLastError(), "wavefront fold launch");
+    return 3;
+}
+
+}  // namespace
+
 int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
                          wf::StageTimes* stages, cudaStream_t stream) {
     if (p.sample_count <= 0 || film.pixels <= 0) return 0;
     State& st = *state_;
-    WfArgs a;
-    a.s = s;
-    a.film = film;
-    a.pool = st.pool;
-    a.capacity = capacity_;
-    a.pixels = film.pixels;
-    a.first_sample = p.first_sample;
-    a.sample_count = p.sample_count;
     // Enough units to fill the pool: split a pixel's samples when pixels < slots.
     int chunks = 1;
     if (film.pixels < capacity_) chunks = std::min(p.sample_count, (capacity_ + film.pixels - 1) / film.pixels);
-    a.chunk = (p.sample_count + chunks - 1) / chunks;
-    a.chunks = (p.sample_count + a.chunk - 1) / a.chunk;
-    a.lbuf = nullptr;
-    if (a.chunks > 1) {
+    WfArgs a{};
+    a.job0 = make_job(s, film, nullptr, p.first_sample, p.sample_count, chunks, p.seed, p.max_depth);
+    if (a.job0.chunks > 1) {
         const size_t need = 3 * (size_t)film.pixels * (size_t)p.sample_count;
         if (need > st.lbuf_floats) {
             if (st.lbuf) cudaFree(st.lbuf);
@@ -626,30 +662,24 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
             cuda_check(cudaMalloc(&st.lbuf, need * sizeof(float)), "cudaMalloc wavefront sample buffer");
             st.lbuf_floats = need;
         }
-        a.lbuf = st.lbuf;
+        a.job0.lbuf = st.lbuf;
     }
-    a.seed = p.seed;
-    a.max_depth = p.max_depth;
+    a.jobs = nullptr;
+    a.hdr = nullptr;
+    a.pool = st.pool;
+    a.capacity = capacity_;
     a.qcap = (p.queue_capacity > 0 && p.queue_capacity < capacity_) ? (uint32_t)p.queue_capacity : (uint32_t)capacity_;
     a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = p.stage_timing ? 1 : 0;
-    Control* ctl = st.pool.ctl;
-    cuda_check(cudaMemsetAsync(ctl, 0, sizeof(Control), stream), "memset control");
-    cuda_check(cudaMemsetAsync(st.pool.status, 0, ((size_t)capacity_ / kWfBlock + 2) * sizeof(unsigned long long),
-                               stream), "memset status");
-    wavefront_init<<<(capacity_ + 255) / 256, 256, 0, stream>>>(st.pool, capacity_);
-    cuda_check(cudaGetLastError(), "wavefront init launch");
-    void* args[] = {&a};
-    cuda_check(cudaLaunchCooperativeKernel((const void*)wavefront_persistent, dim3(st.grid), dim3(kWfBlock), args, 0,
-                                           stream),
-               "wavefront cooperative launch");
-    if (a.chunks > 1) launch_film_commit(film, a.lbuf, p.sample_count, stream);
-    wavefront_fold<<<1, 1, 0, stream>>>(ctl, counters, p.count_rays ? 1 : 0);
-    cuda_check(cudaGetLastError(), "wavefront fold launch");
+    int launches = launch_pool<false>(a, st.grid, capacity_, counters, p.count_rays, stream);
+    if (a.job0.chunks > 1) {
+        launch_film_commit(film, a.job0.lbuf, p.sample_count, stream);
+        ++launches;
+    }
     if (stages) {
         unsigned long long ns[kStages];
-        cuda_check(cudaMemcpyAsync(ns, ctl->stage_ns, sizeof(ns), cudaMemcpyDeviceToHost, stream), "stage times");
+        cuda_check(cudaMemcpyAsync(ns, st.pool.ctl->stage_ns, sizeof(ns), cudaMemcpyDeviceToHost, stream), "stage times");
         cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
         stages->extend += ns[0] * 1e-6;
         stages->classify += ns[1] * 1e-6;
@@ -660,7 +690,21 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
         stages->compact += ns[6] * 1e-6;
         stages->other += ns[7] * 1e-6;
     }
-    return a.chunks > 1 ? 4 : 3;
+    return launches;
+}
+
+int WavefrontEngine::run_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, DevCounters* counters,
+                               bool count_rays, cudaStream_t stream) {
+    WfArgs a{};
+    a.jobs = d_jobs;
+    a.hdr = d_hdr;
+    a.pool = state_->pool;
+    a.capacity = capacity_;
+    a.qcap = (uint32_t)capacity_;
+    a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
+    a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
+    a.split_shading = 0;
+    return launch_pool<true>(a, state_->grid_multi, capacity_, counters, count_rays, stream);
 }
 
 }  // namespace wfb

@@ -18,6 +18,11 @@ public:
     // returns the number of kernels launched.
     int run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
              wf::StageTimes* stages, cudaStream_t stream);
+    // Batch: every job of a device job table (units numbered across jobs, as for the batch
+    // megakernel) in one cooperative launch; the caller commits split-mode films afterwards
+    // (launch_film_commit_jobs). Returns the number of kernels launched.
+    int run_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, DevCounters* counters, bool count_rays,
+                  cudaStream_t stream);
     uint64_t bytes() const;
     int capacity() const { return capacity_; }
 

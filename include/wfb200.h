@@ -195,9 +195,19 @@ int wfb_autotune(wfb_scene_t scene, int width, int height, int probe_spp, int ma
 int wfb_renderer_apply_tuning(wfb_renderer_t r, const wfb_tune_result* t);
 
 /* ---- batched rendering (no reference counterpart: one scene/camera/job per GpuRenderer) -------
- * Many jobs of uneven size rendered in ONE persistent launch, replayed through a CUDA graph
- * captured once per launch shape. Every job's film is bit-identical to the same job rendered
- * alone by wfb_renderer_render. */
+ * Many jobs of uneven size rendered in ONE persistent launch of either arm: the megakernel
+ * (replayed through a CUDA graph captured once per launch shape) or the wavefront (the paths of
+ * every job in one pool, each slot carrying its job). Every job's film is bit-identical to the same
+ * job rendered alone by wfb_renderer_render. */
+typedef struct {
+    int mode;            /* WFB_MODE_MEGAKERNEL or WFB_MODE_WAVEFRONT */
+    int use_graph;       /* megakernel: replay one captured CUDA graph per launch shape */
+    int block;           /* megakernel: 64, 128 or 256 threads; <= 0: 128 */
+    int occupancy;       /* megakernel, block 128: 0, 6 or 8 CTAs per SM by a register cap; < 0: 8 */
+    int min_active;      /* 1..32; <= 0: default */
+    int leaf_batch;      /* 1..32; <= 0: default (see wfb_renderer_configure) */
+    int paths_in_flight; /* wavefront pool slots; <= 0: 1M */
+} wfb_launch_config;
 typedef struct wfb_batch* wfb_batch_t;
 typedef struct {
     float cam_position[3], cam_look_at[3], cam_up[3];
@@ -207,8 +217,8 @@ typedef struct {
     uint32_t seed;
     int max_depth;
 } wfb_job_desc;
-/* use_graph != 0: replay one captured graph per launch shape. block/min_active <= 0: defaults. */
-int wfb_batch_create(int max_jobs, int use_graph, int block, int min_active, wfb_batch_t* out);
+/* cfg NULL: megakernel with graph replay and default knobs. */
+int wfb_batch_create(int max_jobs, const wfb_launch_config* cfg, wfb_batch_t* out);
 int wfb_batch_add(wfb_batch_t b, wfb_scene_t scene, const wfb_job_desc* job, int* job_id);
 int wfb_batch_clear(wfb_batch_t b);
 /* Zeroes all films, renders every job in one launch, waits; stats may be NULL. */
@@ -231,8 +241,7 @@ typedef struct {
     double launch_target_ms; /* 0: 20 */
     int fixed_slice;         /* > 0: samples per job per launch */
     int one_job_per_launch;
-    int use_graph;
-    int block, min_active;   /* <= 0: defaults */
+    wfb_launch_config launch; /* arm and knobs of every launch */
 } wfb_server_config;
 typedef struct {
     uint64_t submitted, completed, cancelled, failed, launches, samples_done;

@@ -43,7 +43,8 @@ def test_abi_version_and_errors(wfb):
 STRUCTS = [("wfb_scene_desc", "SceneDesc"), ("wfb_scene_info", "SceneInfo"),
            ("wfb_render_params", "_CRenderParams"), ("wfb_render_stats", "_CRenderStats"),
            ("wfb_tune_result", "_CTuneResult"), ("wfb_job_desc", "_CJobDesc"),
-           ("wfb_server_config", "_CServerConfig"), ("wfb_server_stats", "_CServerStats")]
+           ("wfb_server_config", "_CServerConfig"), ("wfb_server_stats", "_CServerStats"),
+           ("wfb_launch_config", "_CLaunchConfig")]
 
 
 def test_ctypes_mirrors_match_c_layout(wfb, tmp_path):
