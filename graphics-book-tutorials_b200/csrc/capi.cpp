@@ -130,6 +130,7 @@ wfb::LaunchConfig launch_config(const wfb_launch_config* c) {
     if (c->block > 0) l.mk.block = c->block;
     need(l.mk.block == 64 || l.mk.block == 128 || l.mk.block == 256, "block must be 64, 128 or 256");
     if (c->occupancy >= 0) l.mk.occupancy = c->occupancy;
+    else if (l.mk.block != 128) l.mk.occupancy = 0;  // the register-cap targets exist for block 128 only
     need(l.mk.occupancy == 0 || ((l.mk.occupancy == 6 || l.mk.occupancy == 8) && l.mk.block == 128),
          "occupancy target must be 0, 6 or 8 (block 128)");
     need(c->min_active <= 32 && c->leaf_batch <= 32, "min_active and leaf_batch must be in 1..32");

@@ -52,6 +52,39 @@ def test_batch_jobs_equal_solo_renders(wfb, scenes):
         assert np.array_equal(bits(got.lum_var), bits(want.lum_var))
 
 
+@pytest.mark.parametrize("pool", [1 << 12, 1 << 20])
+def test_wavefront_batch_jobs_equal_solo_renders(wfb, scenes, pool):
+    """Config 4 on the other arm: the paths of every job share one persistent wavefront pool (each
+    slot carries its job); small pools force split jobs and slot reuse across jobs."""
+    jobs = small_jobs(wfb, scenes, 12, seed=7)
+    b = wfb.Batch(max_jobs=16, mode=wfb.WAVEFRONT, paths_in_flight=pool)
+    ids = [b.add(s, j) for s, j in jobs]
+    st = b.run(count_rays=True)
+    assert st.extension_rays > 0 and st.invalid_hits == 0 and st.queue_overflows == 0
+    assert st.kernel_launches == 4
+    mk = wfb.Batch(max_jobs=16)
+    for s, j in jobs:
+        mk.add(s, j)
+    mst = mk.run(count_rays=True)
+    assert (mst.extension_rays, mst.shadow_rays) == (st.extension_rays, st.shadow_rays)
+    for jid, (s, j) in zip(ids, jobs):
+        got = b.download(jid)
+        want = solo(wfb, s, j)
+        assert np.array_equal(bits(got.rgb), bits(want.rgb)), f"job {jid} differs from its solo render"
+        assert np.array_equal(bits(got.lum_var), bits(want.lum_var))
+
+
+def test_wavefront_server_results_equal_solo_renders(wfb, scenes):
+    jobs = small_jobs(wfb, scenes, 6, seed=11)
+    srv = wfb.Server(mode=wfb.WAVEFRONT, paths_in_flight=1 << 18, launch_target_ms=5.0)
+    tickets = [srv.submit(s, j) for s, j in jobs]
+    for t, (s, j) in zip(tickets, jobs):
+        assert srv.wait(t, 60000)
+        res, _ = srv.result(t)
+        assert np.array_equal(bits(res.rgb), bits(solo(wfb, s, j).rgb))
+    srv.close()
+
+
 def test_graph_replay_with_changing_batches(wfb, scenes):
     b = wfb.Batch(max_jobs=16, use_graph=True)
     nog = wfb.Batch(max_jobs=16, use_graph=False)
