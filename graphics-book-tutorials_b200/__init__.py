@@ -529,13 +529,13 @@ class _CJobDesc(ctypes.Structure):
 class _CLaunchConfig(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("use_graph", ctypes.c_int), ("block", ctypes.c_int),
                 ("occupancy", ctypes.c_int), ("min_active", ctypes.c_int), ("leaf_batch", ctypes.c_int),
-                ("paths_in_flight", ctypes.c_int)]
+                ("paths_in_flight", ctypes.c_int), ("split_chunks", ctypes.c_int)]
 
 
 def _launch_config(mode=0, use_graph=True, block=0, occupancy=-1, min_active=0, leaf_batch=0,
-                   paths_in_flight=0) -> _CLaunchConfig:
+                   paths_in_flight=0, split_chunks=0) -> _CLaunchConfig:
     return _CLaunchConfig(int(mode), int(bool(use_graph)), int(block), int(occupancy), int(min_active),
-                          int(leaf_batch), int(paths_in_flight))
+                          int(leaf_batch), int(paths_in_flight), int(split_chunks))
 
 
 class _CServerConfig(ctypes.Structure):
@@ -607,12 +607,14 @@ class Batch:
     """Many jobs in one persistent launch (wfb_batch_*); every job's film equals its solo render."""
 
     def __init__(self, max_jobs: int = 64, use_graph: bool = True, block: int = 0, min_active: int = 0,
-                 mode: int = MEGAKERNEL, occupancy: int = -1, leaf_batch: int = 0, paths_in_flight: int = 0):
+                 mode: int = MEGAKERNEL, occupancy: int = -1, leaf_batch: int = 0, paths_in_flight: int = 0,
+                 split_chunks: int = 0):
         """mode MEGAKERNEL (graph replay when use_graph) or WAVEFRONT (pool of paths_in_flight slots);
         knobs <= 0 (occupancy < 0) keep the defaults."""
         lib = _bind_batch_server(load_library())
         h = ctypes.c_void_p()
-        cfg = _launch_config(mode, use_graph, block, occupancy, min_active, leaf_batch, paths_in_flight)
+        cfg = _launch_config(mode, use_graph, block, occupancy, min_active, leaf_batch, paths_in_flight,
+                             split_chunks)
         _check(lib.wfb_batch_create(int(max_jobs), ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
         self._jobs = []
@@ -668,11 +670,12 @@ class Server:
     def __init__(self, budget_bytes: int = 0, max_jobs: int = 0, launch_target_ms: float = 0.0,
                  fixed_slice: int = 0, one_job_per_launch: bool = False, use_graph: bool = True, block: int = 0,
                  min_active: int = 0, mode: int = MEGAKERNEL, occupancy: int = -1, leaf_batch: int = 0,
-                 paths_in_flight: int = 0):
+                 paths_in_flight: int = 0, split_chunks: int = 0):
         lib = _bind_batch_server(load_library())
         cfg = _CServerConfig(int(budget_bytes), int(max_jobs), float(launch_target_ms), int(fixed_slice),
                              int(bool(one_job_per_launch)),
-                             _launch_config(mode, use_graph, block, occupancy, min_active, leaf_batch, paths_in_flight))
+                             _launch_config(mode, use_graph, block, occupancy, min_active, leaf_batch, paths_in_flight,
+                                            split_chunks))
         h = ctypes.c_void_p()
         _check(lib.wfb_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

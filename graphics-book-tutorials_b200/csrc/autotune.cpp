@@ -6,7 +6,7 @@
 // renders the same film bits (launch knobs never change the arithmetic), so tuning is purely a
 // speed decision. Results are cached per (scene hash, width, height, probe_spp, max_depth).
 // The result holds the best knobs of each arm, so a renderer of either arm can apply it.
-//   megakernel: stage 1, (block, occupancy target) in {(128,8), (128,6), (128,0), (64,0), (256,0)}
+//   megakernel: stage 1, (block, occupancy target) in {(128,10), (128,8), (128,6), (128,0), (64,0), (256,0)}
 //               x min_active in {8, 16, 24} at leaf_batch 8; stage 2, the stage-1 winner with
 //               leaf_batch in {4, 12, 16, 32}
 //   wavefront:  paths in flight in {512K, 1M, 2M} x min_active {16, 24}; its queues are sized to
@@ -58,7 +58,7 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
     {
         Renderer r(scene, wf::GpuMode::Megakernel);
         r.set_camera(cam, width, height);
-        const int shapes[][2] = {{128, 8}, {128, 6}, {128, 0}, {64, 0}, {256, 0}};
+        const int shapes[][2] = {{128, 10}, {128, 8}, {128, 6}, {128, 0}, {64, 0}, {256, 0}};
         const int actives[] = {8, 16, 24};
         best.leaf_batch = 8;
         for (const auto& sh : shapes)

@@ -64,6 +64,9 @@ BatchLauncher::~BatchLauncher() {
 }
 
 int BatchLauncher::chunks_for(int pixels, int samples) const {
+    // Megakernel: the single-render rule (one sample per unit while the job's buffer fits).
+    if (!wf_) return megakernel_split_chunks(pixels, samples, cfg_.mk);
+    // Wavefront: split a job's samples only when its pixels alone cannot fill the pool.
     if (samples <= 1 || pixels >= resident_lanes_) return 1;
     const long long k = ((long long)resident_lanes_ + pixels - 1) / pixels;
     return (int)std::min<long long>(k, samples);
@@ -84,10 +87,23 @@ void BatchLauncher::launch(const std::vector<JobSpec>& jobs, const std::vector<J
         desc[i] = make_job(view, bufs[i].film, bufs[i].lbuf, j.first_sample, j.sample_count, bufs[i].chunks, j.seed,
                            j.max_depth);
     }
-    // Longest units first: they start early and the short ones fill the tail.
-    std::vector<int> order((size_t)n);
+    // Longest units first: they start early and the short ones fill the tail. Among equal unit
+    // lengths, jobs of one scene run together (scenes in order of first appearance), so the L2
+    // holds one scene's BVH at a time instead of every scene's at once.
+    std::vector<int> order((size_t)n), group((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        group[i] = i;
+        for (int k = 0; k < i; ++k)
+            if (desc[k].s.nodes == desc[i].s.nodes) {
+                group[i] = group[k];
+                break;
+            }
+    }
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return desc[x].chunk > desc[y].chunk; });
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        if (desc[x].chunk != desc[y].chunk) return desc[x].chunk > desc[y].chunk;
+        return group[x] < group[y];
+    });
     BatchHeader* hdr = static_cast<BatchHeader*>(h_pinned_);
     JobDesc* table = reinterpret_cast<JobDesc*>(static_cast<char*>(h_pinned_) + sizeof(BatchHeader));
     unsigned long long units = 0;

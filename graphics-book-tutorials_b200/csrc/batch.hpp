@@ -38,7 +38,7 @@ public:
 
     int max_jobs() const { return max_jobs_; }
     const LaunchConfig& config() const { return cfg_; }
-    // Work units per pixel for a job of `pixels` pixels and `samples` samples (split small jobs).
+    // Work units per pixel for a job of `pixels` pixels and `samples` samples.
     int chunks_for(int pixels, int samples) const;
     // Kernels launched by the last launch().
     int last_launches() const { return last_launches_; }

@@ -120,6 +120,9 @@ void need(bool ok, const char* msg) {
     if (!ok) throw wfb::Error(WFB_ERR_INVALID_ARGUMENT, msg);
 }
 
+// Register-cap occupancy targets compiled for block 128 (CTAs per SM).
+bool occupancy_target(int occ) { return occ == 6 || occ == 8 || occ == 10; }
+
 // wfb_launch_config -> LaunchConfig; NULL or values <= 0 (occupancy < 0) keep the defaults.
 wfb::LaunchConfig launch_config(const wfb_launch_config* c) {
     wfb::LaunchConfig l;
@@ -131,12 +134,13 @@ wfb::LaunchConfig launch_config(const wfb_launch_config* c) {
     need(l.mk.block == 64 || l.mk.block == 128 || l.mk.block == 256, "block must be 64, 128 or 256");
     if (c->occupancy >= 0) l.mk.occupancy = c->occupancy;
     else if (l.mk.block != 128) l.mk.occupancy = 0;  // the register-cap targets exist for block 128 only
-    need(l.mk.occupancy == 0 || ((l.mk.occupancy == 6 || l.mk.occupancy == 8) && l.mk.block == 128),
-         "occupancy target must be 0, 6 or 8 (block 128)");
+    need(l.mk.occupancy == 0 || (occupancy_target(l.mk.occupancy) && l.mk.block == 128),
+         "occupancy target must be 0, 6, 8 or 10 (block 128)");
     need(c->min_active <= 32 && c->leaf_batch <= 32, "min_active and leaf_batch must be in 1..32");
     if (c->min_active > 0) l.mk.min_active = l.wf.min_active = c->min_active;
     if (c->leaf_batch > 0) l.mk.leaf_batch = l.wf.leaf_batch = c->leaf_batch;
     if (c->paths_in_flight > 0) l.wf.paths_in_flight = c->paths_in_flight;
+    if (c->split_chunks > 0) l.mk.split_chunks = c->split_chunks;
     return l;
 }
 
@@ -396,8 +400,8 @@ int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int m
         need(r != nullptr, "null renderer");
         need(block <= 0 || block == 64 || block == 128 || block == 256, "block must be 64, 128 or 256");
         need(min_active <= 32, "min_active must be in 1..32");
-        need(occupancy < 0 || occupancy == 0 || ((occupancy == 6 || occupancy == 8) && (block <= 0 || block == 128)),
-             "occupancy target must be 0, 6 or 8 (block 128)");
+        need(occupancy < 0 || occupancy == 0 || (occupancy_target(occupancy) && (block <= 0 || block == 128)),
+             "occupancy target must be 0, 6, 8 or 10 (block 128)");
         need(leaf_batch <= 32, "leaf_batch must be in 1..32");
         r->r->configure(block, blocks_per_sm, min_active, split_chunks, paths_in_flight, occupancy, leaf_batch);
     });

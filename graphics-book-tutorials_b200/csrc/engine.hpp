@@ -53,10 +53,16 @@ struct MegakernelConfig {
     int block = 128;        // threads per CTA (64, 128 or 256)
     int blocks_per_sm = 0;  // 0: as many as fit
     int min_active = 24;    // traverse on while at least this many lanes of a warp traverse
-    int split_chunks = 0;   // work units per pixel; 0: chosen from pixels vs resident lanes
-    int occupancy = 8;      // block 128 only: 6 or 8 caps registers for that many CTAs per SM (0: none)
+    int split_chunks = 0;   // work units per pixel; 0: one sample per unit while its buffer fits
+    int occupancy = 10;     // block 128 only: 6, 8 or 10 caps registers for that many CTAs per SM (0: none)
     int leaf_batch = 8;     // a warp tests primitives once this many lanes hold a pending leaf
 };
+// Split mode keeps each path's radiance (3 floats) per (pixel, sample) until the ordered commit;
+// automatic splitting keeps that buffer under kSplitBufferBytes (renders above it run in sub-passes).
+constexpr uint64_t kSplitBufferBytes = 2ull << 30;
+inline uint64_t split_buffer_bytes(long long pixels, long long samples) {
+    return 3ull * sizeof(float) * (uint64_t)pixels * (uint64_t)samples;
+}
 // Resident threads of the persistent megakernel for this configuration.
 int megakernel_resident_threads(const MegakernelConfig& cfg);
 // Work units per pixel (1 = direct film accumulation; > 1 needs a per-sample buffer).
@@ -127,7 +133,13 @@ struct WavefrontConfig {
 // Launch configuration of a batch or a server: the arm and its knobs.
 struct LaunchConfig {
     wf::GpuMode mode = wf::GpuMode::Megakernel;
-    MegakernelConfig mk{};
+    // The multi-job megakernel keeps more per-lane state than the single-render one; at the
+    // 10-CTA register cap it spills more, so batches default to 8 CTAs per SM.
+    MegakernelConfig mk = [] {
+        MegakernelConfig c;
+        c.occupancy = 8;
+        return c;
+    }();
     WavefrontConfig wf{};
     bool use_graph = true;  // megakernel: replay one captured graph per launch shape
 };

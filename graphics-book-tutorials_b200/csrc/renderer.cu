@@ -83,18 +83,31 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
     cuda_check(cudaMemsetAsync(counters_, 0, sizeof(DevCounters), stream_), "zero counters");
     cuda_check(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
     if (mode_ == wf::GpuMode::Megakernel) {
-        const int chunks = megakernel_split_chunks(pixels(), p.sample_count, mk_cfg_);
-        if (chunks > 1) {
-            const size_t need = 3 * (size_t)pixels() * (size_t)p.sample_count;
-            if (need > lbuf_floats_) {
-                if (lbuf_) cudaFree(lbuf_);
-                lbuf_ = nullptr;
-                lbuf_floats_ = 0;
-                cuda_check(cudaMalloc(&lbuf_, need * sizeof(float)), "cudaMalloc sample buffer");
-                lbuf_floats_ = need;
+        // Automatic splitting: a render whose per-sample buffer would pass the cap runs as
+        // consecutive sub-passes of sample ranges; each pixel still gets its samples in ascending
+        // order, so the film is the same.
+        int step = p.sample_count;
+        if (mk_cfg_.split_chunks == 0 && p.sample_count > 1 &&
+            split_buffer_bytes(pixels(), p.sample_count) > kSplitBufferBytes)
+            step = (int)std::max<uint64_t>(1, kSplitBufferBytes / split_buffer_bytes(pixels(), 1));
+        last_launches_ = 0;
+        for (int done = 0; done < p.sample_count; done += step) {
+            PassParams q = p;
+            q.first_sample = p.first_sample + done;
+            q.sample_count = std::min(step, p.sample_count - done);
+            const int chunks = megakernel_split_chunks(pixels(), q.sample_count, mk_cfg_);
+            if (chunks > 1) {
+                const size_t need = 3 * (size_t)pixels() * (size_t)q.sample_count;
+                if (need > lbuf_floats_) {
+                    if (lbuf_) cudaFree(lbuf_);
+                    lbuf_ = nullptr;
+                    lbuf_floats_ = 0;
+                    cuda_check(cudaMalloc(&lbuf_, need * sizeof(float)), "cudaMalloc sample buffer");
+                    lbuf_floats_ = need;
+                }
             }
+            last_launches_ += launch_megakernel(view_, film_, counters_, work_, lbuf_, q, mk_cfg_, chunks, stream_);
         }
-        last_launches_ = launch_megakernel(view_, film_, counters_, work_, lbuf_, p, mk_cfg_, chunks, stream_);
     } else {
         last_launches_ = wf_->engine.run(view_, film_, counters_, p, stats ? &stats->stages : nullptr, stream_);
     }

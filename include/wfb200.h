@@ -166,7 +166,7 @@ uint64_t wfb_renderer_device_bytes(wfb_renderer_t r);
 /* Launch configuration knobs (no reference counterpart; set by the autotuner). Any value < 0
  * keeps the current setting. Megakernel: block 64/128/256 threads, CTAs per SM (0: all that fit),
  * the minimum number of traversing lanes per warp before shading runs (1..32), work units per
- * pixel (0: automatic), occupancy target (block 128: 0 none, 6 or 8 CTAs per SM by a register
+ * pixel (0: automatic), occupancy target (block 128: 0 none, 6, 8 or 10 CTAs per SM by a register
  * cap), and leaf_batch (1..32): a warp runs a round of primitive tests once this many of its
  * lanes hold a pending leaf (or they outnumber the lanes testing boxes). Wavefront: paths in
  * flight, min_active and leaf_batch. */
@@ -203,10 +203,12 @@ typedef struct {
     int mode;            /* WFB_MODE_MEGAKERNEL or WFB_MODE_WAVEFRONT */
     int use_graph;       /* megakernel: replay one captured CUDA graph per launch shape */
     int block;           /* megakernel: 64, 128 or 256 threads; <= 0: 128 */
-    int occupancy;       /* megakernel, block 128: 0, 6 or 8 CTAs per SM by a register cap; < 0: 8 */
+    int occupancy;       /* megakernel, block 128: 0, 6, 8 or 10 CTAs per SM by a register cap; < 0: 8 */
     int min_active;      /* 1..32; <= 0: default */
     int leaf_batch;      /* 1..32; <= 0: default (see wfb_renderer_configure) */
     int paths_in_flight; /* wavefront pool slots; <= 0: 1M */
+    int split_chunks;    /* megakernel: work units per pixel of each job; <= 0: automatic (one
+                            sample per unit while the job's per-sample buffer fits) */
 } wfb_launch_config;
 typedef struct wfb_batch* wfb_batch_t;
 typedef struct {
