@@ -519,6 +519,7 @@ int wfb_server_create(const wfb_server_config* c, wfb_server_t* out) {
         cfg.fixed_slice = c->fixed_slice;
         cfg.one_job_per_launch = c->one_job_per_launch != 0;
         cfg.launch = launch_config(&c->launch);
+        if (c->launch.split_chunks <= 0) cfg.launch.mk.split_chunks = wfb::kServerSplitChunks;
         auto s = std::make_unique<wfb_server>();
         s->s = std::make_unique<wfb::Server>(cfg);
         *out = s.release();

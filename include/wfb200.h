@@ -243,7 +243,7 @@ typedef struct {
     double launch_target_ms; /* 0: 20 */
     int fixed_slice;         /* > 0: samples per job per launch */
     int one_job_per_launch;
-    wfb_launch_config launch; /* arm and knobs of every launch */
+    wfb_launch_config launch; /* arm and knobs of every launch (split_chunks <= 0: 4 for servers) */
 } wfb_server_config;
 typedef struct {
     uint64_t submitted, completed, cancelled, failed, launches, samples_done;
