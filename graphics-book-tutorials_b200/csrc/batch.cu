@@ -17,7 +17,7 @@ void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var
     if (spp_done <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "spp_done must be positive");
     const size_t p = (size_t)film.pixels;
     std::vector<float> lum, lum2;
-    cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    if (stream) cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
     if (rgb) cuda_check(cudaMemcpy(rgb, film.rgb, 3 * p * sizeof(float), cudaMemcpyDeviceToHost), "download rgb");
     if (lum_var) {
         lum.resize(p);
@@ -55,9 +55,11 @@ BatchLauncher::BatchLauncher(int max_jobs, const LaunchConfig& cfg) : max_jobs_(
     d_counters_ = reinterpret_cast<DevCounters*>(p + ((table + 255) & ~(size_t)255));
     d_work_ = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(d_counters_) + 256);
     cuda_check(cudaMallocHost(&h_pinned_, table), "cudaMallocHost batch staging");
+    cuda_check(cudaEventCreateWithFlags(&staged_, cudaEventDisableTiming), "cudaEventCreate");
 }
 
 BatchLauncher::~BatchLauncher() {
+    if (staged_) cudaEventDestroy(staged_);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (h_pinned_) cudaFreeHost(h_pinned_);
     if (arena_) cudaFree(arena_);
@@ -77,8 +79,8 @@ void BatchLauncher::launch(const std::vector<JobSpec>& jobs, const std::vector<J
     const int n = (int)jobs.size();
     if (n > max_jobs_) throw Error(WFB_ERR_INVALID_ARGUMENT, "more jobs than the batch holds");
     if (bufs.size() != jobs.size()) throw Error(WFB_ERR_INTERNAL, "job buffers do not match the jobs");
-    // The staging buffer may still feed the previous launch's copy.
-    cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    // The staging buffer may still feed this launcher's previous table upload.
+    cuda_check(cudaEventSynchronize(staged_), "wait for the previous table upload");
     std::vector<JobDesc> desc((size_t)n);
     for (int i = 0; i < n; ++i) {
         const JobSpec& j = jobs[i];
@@ -120,6 +122,7 @@ void BatchLauncher::launch(const std::vector<JobSpec>& jobs, const std::vector<J
     cuda_check(cudaMemcpyAsync(d_hdr_, h_pinned_, sizeof(BatchHeader) + (size_t)n * sizeof(JobDesc),
                                cudaMemcpyHostToDevice, stream),
                "upload job table");
+    cuda_check(cudaEventRecord(staged_, stream), "cudaEventRecord");
     cuda_check(cudaMemsetAsync(d_counters_, 0, sizeof(DevCounters), stream), "zero counters");
     if (wf_) {
         last_launches_ = wf_->run_batch(d_jobs_, d_hdr_, d_counters_, count_rays, stream);

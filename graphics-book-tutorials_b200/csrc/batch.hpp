@@ -43,7 +43,9 @@ public:
     // Kernels launched by the last launch().
     int last_launches() const { return last_launches_; }
     // Enqueues one launch over `jobs` (their films must hold the sums to add to); jobs are
-    // reordered longest-unit-first on the device table only. Returns after enqueueing.
+    // reordered longest-unit-first on the device table only. Returns after enqueueing; it waits
+    // only for this launcher's previous table upload (not for earlier launches), so a caller with
+    // two launchers can prepare one launch while the other runs.
     void launch(const std::vector<JobSpec>& jobs, const std::vector<JobBuffers>& bufs, bool count_rays,
                 cudaStream_t stream);
     // Counters of the last launch (synchronises the stream).
@@ -62,6 +64,7 @@ private:
     DevCounters* d_counters_ = nullptr;
     unsigned* d_work_ = nullptr;
     void* h_pinned_ = nullptr;  // staging for header + table
+    cudaEvent_t staged_ = nullptr;  // recorded after the last table upload: the staging is free again
     cudaGraphExec_t graph_exec_ = nullptr;
     bool count_rays_in_graph_ = false;
 };
@@ -92,7 +95,8 @@ private:
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 };
 
-// Host-side conversions shared by renderers, batches and the server.
+// Host-side conversions shared by renderers, batches and the server. `stream` is synchronised
+// first unless it is null (the caller has already waited for the work that wrote the film).
 void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream);
 
 }  // namespace wfb

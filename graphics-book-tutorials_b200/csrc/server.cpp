@@ -15,6 +15,8 @@
 //    admitting and retiring jobs never blocks the device.
 //  * Plain mode (one_job_per_launch) renders queued jobs one at a time, FIFO, one launch each:
 //    the sequential baseline at the same arrival stream.
+//  * Two launches are in flight: the worker prepares and enqueues the next launch (and copies
+//    finished films) while the GPU renders the current one.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -32,7 +34,10 @@ double now_seconds() {
 struct Server::Job {
     JobSpec spec;
     int state = kQueued;
-    int done = 0;  // samples added to the film so far
+    int done = 0;      // samples added to the film so far (launches finished)
+    int issued = 0;    // samples enqueued (launches finished or in flight)
+    int inflight = 0;  // launches in flight that render some of this job
+    bool downloading = false;  // all samples rendered; the download thread is copying the film
     double t_arrival = 0.0, t_done = 0.0;
     JobBuffers buf;
     void* mem = nullptr;
@@ -42,11 +47,13 @@ struct Server::Job {
 };
 
 Server::Server(const ServerConfig& cfg) : cfg_(cfg) {
+    // Plain mode launches one job at a time but admits two, so that it too keeps one launch in
+    // flight while the previous one is retired.
+    max_active_ = cfg_.one_job_per_launch ? 2 : cfg_.max_jobs;
     if (cfg_.one_job_per_launch) cfg_.max_jobs = 1;
-    launcher_ = std::make_unique<BatchLauncher>(cfg_.max_jobs, cfg_.launch);
+    for (auto& l : launchers_) l = std::make_unique<BatchLauncher>(cfg_.max_jobs, cfg_.launch);
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaEventCreate(&ev0_), "cudaEventCreate");
-    cuda_check(cudaEventCreate(&ev1_), "cudaEventCreate");
+    for (auto& e : ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
     int dev = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     device_ = dev;
@@ -56,6 +63,7 @@ Server::Server(const ServerConfig& cfg) : cfg_(cfg) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     thread_ = std::thread([this] { worker(); });
+    dl_thread_ = std::thread([this] { downloader(); });
 }
 
 Server::~Server() { shutdown(); }
@@ -67,7 +75,9 @@ void Server::shutdown() {
         stop_ = true;
     }
     cv_work_.notify_all();
+    cv_dl_.notify_all();
     if (thread_.joinable()) thread_.join();
+    if (dl_thread_.joinable()) dl_thread_.join();
     std::lock_guard<std::mutex> lock(mu_);
     for (auto& kv : jobs_)
         if (kv.second->mem) {
@@ -79,16 +89,17 @@ void Server::shutdown() {
         cudaStreamDestroy(stream_);
         stream_ = nullptr;
     }
-    if (ev0_) cudaEventDestroy(ev0_);
-    if (ev1_) cudaEventDestroy(ev1_);
-    ev0_ = ev1_ = nullptr;
-    launcher_.reset();
+    for (auto& e : ev_) {
+        if (e) cudaEventDestroy(e);
+        e = nullptr;
+    }
+    for (auto& l : launchers_) l.reset();
     cv_done_.notify_all();
 }
 
 uint64_t Server::job_bytes(const Job& j) const {
     const uint64_t p = (uint64_t)j.spec.width * j.spec.height;
-    const int chunks = launcher_->chunks_for((int)p, j.spec.sample_count);
+    const int chunks = launchers_[0]->chunks_for((int)p, j.spec.sample_count);
     uint64_t b = 5 * p * sizeof(float);
     if (chunks > 1) b += 3 * p * (uint64_t)j.spec.sample_count * sizeof(float);
     return b;
@@ -206,11 +217,11 @@ void Server::reset_stats() {
 // Moves queued jobs to the active set while budget and launch capacity allow (FIFO, no overtaking).
 bool Server::admit_locked() {
     bool any = false;
-    while (!queue_.empty() && (int)active_.size() < cfg_.max_jobs) {
+    while (!queue_.empty() && (int)active_.size() < max_active_) {
         Job& j = *jobs_[queue_.front()];
         if (bytes_in_use_ + j.bytes > cfg_.budget_bytes) break;
         const uint64_t p = (uint64_t)j.spec.width * j.spec.height;
-        j.buf.chunks = launcher_->chunks_for((int)p, j.spec.sample_count);
+        j.buf.chunks = launchers_[0]->chunks_for((int)p, j.spec.sample_count);
         if (cudaMallocAsync(&j.mem, j.bytes, stream_) != cudaSuccess) {
             cudaGetLastError();
             break;  // try again after a job retires
@@ -237,11 +248,11 @@ int Server::choose_slice(const std::vector<Job*>& act) {
     auto total = [&](int k) {
         double s = 0.0;
         for (const Job* j : act)
-            s += (double)j->spec.width * j->spec.height * std::min(k, j->spec.sample_count - j->done);
+            s += (double)j->spec.width * j->spec.height * std::min(k, j->spec.sample_count - j->issued);
         return s;
     };
     int lo = 1, hi = 1;
-    for (const Job* j : act) hi = std::max(hi, j->spec.sample_count - j->done);
+    for (const Job* j : act) hi = std::max(hi, j->spec.sample_count - j->issued);
     while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;
         if (total(mid) <= budget) lo = mid;
@@ -250,116 +261,197 @@ int Server::choose_slice(const std::vector<Job*>& act) {
     return lo;
 }
 
+// Two launches in flight: while the GPU renders launch N, the worker retires launch N-1's
+// finished jobs (film copies overlap launch N) and enqueues launch N+1 on the other launcher, so
+// the device does not idle through host bookkeeping. Slices are planned from `issued` samples;
+// launches on the one stream run in order, so a job's slices still add in ascending sample order.
 void Server::worker() {
     cudaSetDevice(device_);  // the device the server was created on
-    for (;;) {
-        std::vector<Job*> act;
+    struct Flight {
+        std::vector<Job*> jobs;
         std::vector<uint64_t> tickets;
+        std::vector<int> counts;  // samples of each job in this launch
+        uint64_t samples = 0;
+        int slot = 0;
+        std::string err;
+    };
+    std::deque<Flight> flights;
+    int next_slot = 0;
+    for (;;) {
+        Flight f;
         {
             std::unique_lock<std::mutex> lock(mu_);
-            // drop cancelled active jobs
-            for (auto it = active_.begin(); it != active_.end();) {
-                Job& j = *jobs_[*it];
-                if (j.state == kCancelled) {
-                    if (j.mem) cudaFreeAsync(j.mem, stream_);
-                    j.mem = nullptr;
-                    bytes_in_use_ -= j.bytes;
-                    jobs_.erase(*it);
-                    it = active_.erase(it);
-                } else {
-                    ++it;
-                }
-            }
+            release_idle_locked();
             admit_locked();
-            while (active_.empty() && !stop_) {
+            auto issuable = [&] {
+                for (uint64_t t : active_) {
+                    const Job& j = *jobs_[t];
+                    if (j.state == kActive && j.issued < j.spec.sample_count) return true;
+                }
+                return false;
+            };
+            while (!stop_ && flights.empty() && !issuable()) {
                 cv_work_.wait(lock);
+                release_idle_locked();
                 admit_locked();
             }
-            if (stop_) return;
-            for (uint64_t t : active_) {
-                tickets.push_back(t);
-                act.push_back(jobs_[t].get());
+            if (stop_) break;
+            if (flights.size() < 2)
+                for (uint64_t t : active_) {
+                    Job* j = jobs_[t].get();
+                    if (j->state == kActive && j->issued < j->spec.sample_count) {
+                        f.tickets.push_back(t);
+                        f.jobs.push_back(j);
+                        if (cfg_.one_job_per_launch) break;  // the oldest admitted job, whole
+                    }
+                }
+        }
+        if (!f.jobs.empty()) {
+            // ---- enqueue one launch: every issuable job advances by a slice ----
+            const int k = choose_slice(f.jobs);
+            std::vector<JobSpec> specs;
+            std::vector<JobBuffers> bufs;
+            for (Job* j : f.jobs) {
+                JobSpec sp = j->spec;
+                sp.first_sample = j->issued;
+                sp.sample_count = std::min(k, j->spec.sample_count - j->issued);
+                f.samples += (uint64_t)sp.width * sp.height * sp.sample_count;
+                f.counts.push_back(sp.sample_count);
+                JobBuffers b = j->buf;
+                b.chunks = std::min(b.chunks, sp.sample_count);
+                if (b.chunks > 1 && b.lbuf == nullptr) b.chunks = 1;
+                specs.push_back(sp);
+                bufs.push_back(b);
             }
+            f.slot = next_slot;
+            next_slot ^= 1;
+            try {
+                cuda_check(cudaEventRecord(ev_[2 * f.slot], stream_), "cudaEventRecord");
+                launchers_[f.slot]->launch(specs, bufs, false, stream_);
+                cuda_check(cudaEventRecord(ev_[2 * f.slot + 1], stream_), "cudaEventRecord");
+            } catch (const std::exception& e) {
+                f.err = e.what();
+            }
+            {
+                std::lock_guard<std::mutex> lock(mu_);
+                for (size_t i = 0; i < f.jobs.size(); ++i) {
+                    f.jobs[i]->issued += f.counts[i];
+                    f.jobs[i]->inflight++;
+                }
+            }
+            flights.push_back(std::move(f));
+            if (flights.size() < 2) continue;  // fill the pipeline before waiting
         }
-        // ---- one launch: every active job advances by a slice ----
-        const int k = choose_slice(act);
-        std::vector<JobSpec> specs;
-        std::vector<JobBuffers> bufs;
-        uint64_t samples = 0;
-        for (Job* j : act) {
-            JobSpec s = j->spec;
-            s.first_sample = j->done;
-            s.sample_count = std::min(k, j->spec.sample_count - j->done);
-            samples += (uint64_t)s.width * s.height * s.sample_count;
-            JobBuffers b = j->buf;
-            b.chunks = std::min(b.chunks, s.sample_count);
-            if (b.chunks > 1 && b.lbuf == nullptr) b.chunks = 1;
-            specs.push_back(s);
-            bufs.push_back(b);
-        }
-        std::string err;
+        if (flights.empty()) continue;
+        // ---- retire the oldest launch ----
+        Flight done = std::move(flights.front());
+        flights.pop_front();
         float ms = 0.f;
-        try {
-            cuda_check(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
-            launcher_->launch(specs, bufs, false, stream_);
-            cuda_check(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
-            cuda_check(cudaEventSynchronize(ev1_), "server launch");
-            cudaEventElapsedTime(&ms, ev0_, ev1_);
-        } catch (const std::exception& e) {
-            err = e.what();
+        if (done.err.empty()) {
+            const cudaError_t e = cudaEventSynchronize(ev_[2 * done.slot + 1]);
+            if (e != cudaSuccess) done.err = cudaGetErrorString(e);
+            else cudaEventElapsedTime(&ms, ev_[2 * done.slot], ev_[2 * done.slot + 1]);
         }
-        if (err.empty() && ms > 0.f && samples > 0) {
-            const double rate = (double)samples / (ms * 1e3);  // Msamples/s
+        // Only launches that filled most of their budget refine the rate: a launch carrying a few
+        // small jobs is dominated by its ramp-up and tail, and its low rate would shrink every
+        // following slice (large jobs would then crawl through many short launches).
+        const double budget = msps_estimate_ * 1e3 * cfg_.launch_target_ms;
+        if (done.err.empty() && ms > 0.f && (double)done.samples >= 0.5 * budget) {
+            const double rate = (double)done.samples / (ms * 1e3);  // Msamples/s
             msps_estimate_ = 0.7 * msps_estimate_ + 0.3 * rate;
         }
-        // ---- retire finished jobs: download outside the lock, then update states under it ----
-        std::vector<char> over(act.size(), 0);
-        for (size_t i = 0; i < act.size(); ++i) {
-            Job* j = act[i];
-            if (!err.empty()) {
-                over[i] = 1;
-                continue;
-            }
-            j->done += specs[i].sample_count;
-            if (j->done < j->spec.sample_count) continue;
-            over[i] = 1;
-            const size_t p = (size_t)j->spec.width * j->spec.height;
-            j->rgb.resize(3 * p);
-            j->lum_var.resize(p);
-            try {
-                film_download(j->buf.film, j->spec.sample_count, j->rgb.data(), j->lum_var.data(), stream_);
-            } catch (const std::exception& e) {
-                if (err.empty()) err = e.what();
-            }
-        }
+        // Jobs this launch finished go to the download thread: no later launch touches their films,
+        // so the copies overlap the launch in flight and the worker goes on enqueueing.
+        bool handed = false;
         {
             std::lock_guard<std::mutex> lock(mu_);
             st_.launches++;
             st_.busy_ms += ms;
-            st_.samples_done += samples;
-            const double t = now_seconds();
-            for (size_t i = 0; i < act.size(); ++i) {
-                if (!over[i]) continue;
-                Job* j = act[i];
-                if (j->mem) cudaFreeAsync(j->mem, stream_);
-                j->mem = nullptr;
-                bytes_in_use_ -= j->bytes;
-                active_.erase(std::remove(active_.begin(), active_.end(), tickets[i]), active_.end());
-                if (j->state == kCancelled) {
-                    jobs_.erase(tickets[i]);  // nobody waits for a cancelled job's film
-                } else if (!err.empty()) {
+            st_.samples_done += done.samples;
+            for (size_t i = 0; i < done.jobs.size(); ++i) {
+                Job* j = done.jobs[i];
+                j->inflight--;
+                j->done += done.counts[i];
+                if (j->state != kActive) continue;  // cancelled meanwhile: released when idle
+                if (!done.err.empty()) {
+                    j->state = kFailed;
+                    j->error = done.err;
+                    st_.failed++;
+                } else if (j->done >= j->spec.sample_count) {
+                    j->downloading = true;
+                    dl_queue_.push_back(done.tickets[i]);
+                    handed = true;
+                }
+            }
+            release_idle_locked();
+        }
+        if (handed) cv_dl_.notify_one();
+        cv_done_.notify_all();
+    }
+    // stopping: let launches in flight finish before their memory is released
+    cudaStreamSynchronize(stream_);
+}
+
+// Copies the films of finished jobs to the host (GPU-arm download convention) and completes them.
+// The film is final: its job's last launch has finished and no later launch renders it.
+void Server::downloader() {
+    cudaSetDevice(device_);
+    for (;;) {
+        uint64_t ticket;
+        Job* j;
+        {
+            std::unique_lock<std::mutex> lock(mu_);
+            cv_dl_.wait(lock, [&] { return stop_ || !dl_queue_.empty(); });
+            if (dl_queue_.empty()) return;  // stopping with nothing left to copy
+            ticket = dl_queue_.front();
+            dl_queue_.pop_front();
+            j = jobs_[ticket].get();
+        }
+        const size_t p = (size_t)j->spec.width * j->spec.height;
+        std::string err;
+        try {
+            j->rgb.resize(3 * p);
+            j->lum_var.resize(p);
+            film_download(j->buf.film, j->spec.sample_count, j->rgb.data(), j->lum_var.data(), nullptr);
+        } catch (const std::exception& e) {
+            err = e.what();
+        }
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            j->downloading = false;
+            if (j->state == kActive) {
+                if (err.empty()) {
+                    j->state = kDone;
+                    j->t_done = now_seconds();
+                    st_.completed++;
+                    latencies_ms_.push_back(1e3 * (j->t_done - j->t_arrival));
+                } else {
                     j->state = kFailed;
                     j->error = err;
                     st_.failed++;
-                } else {
-                    j->state = kDone;
-                    j->t_done = t;
-                    st_.completed++;
-                    latencies_ms_.push_back(1e3 * (t - j->t_arrival));
                 }
             }
+            release_idle_locked();  // frees the film's device memory (and forgets a cancelled job)
         }
         cv_done_.notify_all();
+        cv_work_.notify_one();  // memory came back: more jobs may be admitted
+    }
+}
+
+// Frees the device memory of jobs that left the active set (done, failed or cancelled) once no
+// launch in flight renders them; cancelled jobs are forgotten, finished ones wait for result().
+void Server::release_idle_locked() {
+    for (auto it = active_.begin(); it != active_.end();) {
+        Job& j = *jobs_[*it];
+        if (j.state == kActive || j.inflight > 0 || j.downloading) {
+            ++it;
+            continue;
+        }
+        if (j.mem) cudaFreeAsync(j.mem, stream_);
+        j.mem = nullptr;
+        bytes_in_use_ -= j.bytes;
+        if (j.state == kCancelled) jobs_.erase(*it);
+        it = active_.erase(it);
     }
 }
 

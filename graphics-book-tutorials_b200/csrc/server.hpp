@@ -62,22 +62,28 @@ private:
     void worker();
     uint64_t job_bytes(const Job& j) const;
     bool admit_locked();
+    void release_idle_locked();
+    void downloader();
     int choose_slice(const std::vector<Job*>& act);
 
     ServerConfig cfg_;
-    std::unique_ptr<BatchLauncher> launcher_;
+    std::unique_ptr<BatchLauncher> launchers_[2];  // alternate launches: one renders, one is prepared
     cudaStream_t stream_ = nullptr;
-    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};  // start / end of each launcher's launch
     std::mutex mu_;
     std::condition_variable cv_work_, cv_done_;
     std::map<uint64_t, std::unique_ptr<Job>> jobs_;
     std::deque<uint64_t> queue_;
     std::vector<uint64_t> active_;
     uint64_t next_ticket_ = 1;
+    int max_active_ = 256;  // admitted jobs at once
     bool stop_ = false;
     std::thread thread_;
+    std::thread dl_thread_;               // copies finished films to the host
+    std::condition_variable cv_dl_;
+    std::deque<uint64_t> dl_queue_;
     uint64_t bytes_in_use_ = 0, peak_bytes_ = 0;
-    double msps_estimate_ = 200.0;  // Msamples/s, refined after every launch
+    double msps_estimate_ = 500.0;  // Msamples/s, refined by launches that filled their budget
     std::vector<double> latencies_ms_;
     ServerStats st_;
     double t_first_ = -1.0;
