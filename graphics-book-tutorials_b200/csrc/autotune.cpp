@@ -9,7 +9,8 @@
 //   megakernel: stage 1, (block, occupancy target) in {(128,10), (128,8), (128,6), (128,0), (64,0), (256,0)}
 //               x min_active in {8, 16, 24} at leaf_batch 8; stage 2, the stage-1 winner with
 //               leaf_batch in {4, 12, 16, 32}
-//   wavefront:  paths in flight in {512K, 1M, 2M} x min_active {16, 24}; its queues are sized to
+//   wavefront:  paths in flight in {1M, 2M, 4M, 8M} x min_active {16, 24}, probed with at least 8
+//               samples so that the pool can fill; its queues are sized to
 //               the pool, so they never drop a path.
 #include <algorithm>
 #include <map>
@@ -85,14 +86,17 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
         }
     }
     if (try_wavefront) {
-        const int pools[] = {1 << 19, 1 << 20, 1 << 21};
+        const int pools[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
         const int actives[] = {16, 24};
+        PassParams pw = p;  // enough samples for the larger pools to fill
+        pw.sample_count = std::max(probe_spp, 8);
+        const double samples_w = (double)width * height * pw.sample_count;
         Renderer r(scene, wf::GpuMode::Wavefront);
         r.set_camera(cam, width, height);
         for (int pool : pools)
             for (int ma : actives) {
                 r.configure(-1, -1, ma, -1, pool, -1);
-                const double ms = measure(r, p);
+                const double ms = measure(r, pw) * samples / samples_w;  // per probe_spp samples
                 best.candidates++;
                 if (ms < wf_ms) {
                     wf_ms = ms;

@@ -68,8 +68,11 @@ BatchLauncher::~BatchLauncher() {
 int BatchLauncher::chunks_for(int pixels, int samples) const {
     // Megakernel: the single-render rule (one sample per unit while the job's buffer fits).
     if (!wf_) return megakernel_split_chunks(pixels, samples, cfg_.mk);
-    // Wavefront: split a job's samples only when its pixels alone cannot fill the pool.
-    if (samples <= 1 || pixels >= resident_lanes_) return 1;
+    // Wavefront: one sample per unit while the job's buffer fits, else split a job's samples only
+    // when its pixels alone cannot fill the pool.
+    if (samples <= 1) return 1;
+    if (split_buffer_bytes(pixels, samples) <= kSplitBufferBytes) return samples;
+    if (pixels >= resident_lanes_) return 1;
     const long long k = ((long long)resident_lanes_ + pixels - 1) / pixels;
     return (int)std::min<long long>(k, samples);
 }

@@ -125,7 +125,7 @@ void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
 
 // ---- wavefront (wavefront.cu) ----
 struct WavefrontConfig {
-    int paths_in_flight = 0;  // path-pool slots; 0: 1M (capped at 64 x pixels)
+    int paths_in_flight = 0;  // path-pool slots; 0: 4M (capped at 64 x pixels)
     int min_active = 20;      // traverse on while at least this many lanes of a warp traverse
     int leaf_batch = 8;       // a warp tests primitives once this many lanes hold a pending leaf
 };

@@ -591,7 +591,7 @@ struct WavefrontEngine::State {
 
 WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixels_(pixels), cfg_(cfg) {
     if (pixels <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "wavefront needs at least one pixel");
-    int cap = cfg.paths_in_flight > 0 ? cfg.paths_in_flight : (1 << 20);
+    int cap = cfg.paths_in_flight > 0 ? cfg.paths_in_flight : (1 << 22);
     if (cap > pixels * 64) cap = pixels * 64;  // never more slots than units can use
     if (cap < 32) cap = 32;
     capacity_ = cap;
@@ -648,9 +648,12 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
                          wf::StageTimes* stages, cudaStream_t stream) {
     if (p.sample_count <= 0 || film.pixels <= 0) return 0;
     State& st = *state_;
-    // Enough units to fill the pool: split a pixel's samples when pixels < slots.
+    // One sample per unit while the per-sample buffer fits (as in the megakernel: consecutive slots
+    // get neighbouring pixels at the same sample, and a slot takes new work after every path);
+    // otherwise split a pixel's samples only as far as needed to fill the pool.
     int chunks = 1;
-    if (film.pixels < capacity_) chunks = std::min(p.sample_count, (capacity_ + film.pixels - 1) / film.pixels);
+    if (split_buffer_bytes(film.pixels, p.sample_count) <= kSplitBufferBytes) chunks = p.sample_count;
+    else if (film.pixels < capacity_) chunks = std::min(p.sample_count, (capacity_ + film.pixels - 1) / film.pixels);
     WfArgs a{};
     a.job0 = make_job(s, film, nullptr, p.first_sample, p.sample_count, chunks, p.seed, p.max_depth);
     if (a.job0.chunks > 1) {

@@ -206,7 +206,7 @@ typedef struct {
     int occupancy;       /* megakernel, block 128: 0, 6, 8 or 10 CTAs per SM by a register cap; < 0: 8 */
     int min_active;      /* 1..32; <= 0: default */
     int leaf_batch;      /* 1..32; <= 0: default (see wfb_renderer_configure) */
-    int paths_in_flight; /* wavefront pool slots; <= 0: 1M */
+    int paths_in_flight; /* wavefront pool slots; <= 0: 4M */
     int split_chunks;    /* megakernel: work units per pixel of each job; <= 0: automatic (one
                             sample per unit while the job's per-sample buffer fits) */
 } wfb_launch_config;
