@@ -134,11 +134,14 @@ void BatchLauncher::launch(const std::vector<JobSpec>& jobs, const std::vector<J
         return;
     }
     last_launches_ = 2;  // persistent megakernel + film commits
+    bool all_split = n > 0;
+    for (int i = 0; i < n; ++i) all_split = all_split && desc[i].chunks > 1;
     if (!cfg_.use_graph) {
-        launch_megakernel_batch(d_jobs_, d_hdr_, max_jobs_, d_counters_, d_work_, count_rays, cfg_.mk, stream);
+        launch_megakernel_batch(d_jobs_, d_hdr_, max_jobs_, d_counters_, d_work_, count_rays, cfg_.mk, all_split,
+                                stream);
         return;
     }
-    if (graph_exec_ && count_rays_in_graph_ != count_rays) {
+    if (graph_exec_ && (count_rays_in_graph_ != count_rays || split_in_graph_ != all_split)) {
         cudaGraphExecDestroy(graph_exec_);
         graph_exec_ = nullptr;
     }
@@ -146,7 +149,8 @@ void BatchLauncher::launch(const std::vector<JobSpec>& jobs, const std::vector<J
         cudaGraph_t graph = nullptr;
         cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
         try {
-            launch_megakernel_batch(d_jobs_, d_hdr_, max_jobs_, d_counters_, d_work_, count_rays, cfg_.mk, stream);
+            launch_megakernel_batch(d_jobs_, d_hdr_, max_jobs_, d_counters_, d_work_, count_rays, cfg_.mk, all_split,
+                                    stream);
         } catch (...) {
             cudaStreamEndCapture(stream, &graph);
             if (graph) cudaGraphDestroy(graph);
@@ -157,6 +161,7 @@ void BatchLauncher::launch(const std::vector<JobSpec>& jobs, const std::vector<J
         cudaGraphDestroy(graph);
         cuda_check(e, "instantiate batch graph");
         count_rays_in_graph_ = count_rays;
+        split_in_graph_ = all_split;
     }
     cuda_check(cudaGraphLaunch(graph_exec_, stream), "launch batch graph");
 }

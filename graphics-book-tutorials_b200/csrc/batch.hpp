@@ -67,6 +67,7 @@ private:
     cudaEvent_t staged_ = nullptr;  // recorded after the last table upload: the staging is free again
     cudaGraphExec_t graph_exec_ = nullptr;
     bool count_rays_in_graph_ = false;
+    bool split_in_graph_ = false;  // the captured graph runs the all-split kernel variant
 };
 
 // Synchronous batch API (wfb_batch_*): owns the films of its jobs.

@@ -118,10 +118,11 @@ __device__ __forceinline__ int job_of_unit(const JobDesc* jobs, int n_jobs, unsi
 void launch_film_commit_jobs(const JobDesc* d_jobs, const BatchHeader* d_hdr, int max_jobs, cudaStream_t stream);
 // Persistent megakernel over a device job table (unit_begin must be the running sum of units)
 // followed by the split-mode commits of its jobs; max_jobs bounds the job count of any batch
-// replayed through the same launch. Stream-ordered, no host synchronisation, capturable.
+// replayed through the same launch; all_split: every job has chunks > 1 (the leaner kernel variant).
+// Stream-ordered, no host synchronisation, capturable.
 void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, int max_jobs, DevCounters* counters,
                              unsigned int* work_counter, bool count_rays, const MegakernelConfig& cfg,
-                             cudaStream_t stream);
+                             bool all_split, cudaStream_t stream);
 
 // ---- wavefront (wavefront.cu) ----
 struct WavefrontConfig {

@@ -61,7 +61,9 @@ __device__ __forceinline__ const JobDesc& job_at(const MkArgs& a, int j) {
 
 // MINB > 1 caps registers so that MINB CTAs fit an SM (__launch_bounds__ minimum blocks).
 // COUNT adds node-visit and primitive-test counters (used by count_rays runs only).
-template <int BLOCK, bool MULTI, int MINB, bool COUNT>
+// SPLIT: every job of the launch is in split mode (chunks > 1), so the per-lane film accumulators
+// of direct mode and their branches are compiled out (5 registers fewer under the register cap).
+template <int BLOCK, bool MULTI, int MINB, bool COUNT, bool SPLIT>
 __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArgs a) {
     const int lane = threadIdx.x & 31;
     const unsigned total_units = MULTI ? a.hdr->total_units : a.job0.units;
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
                 }
             }
             if (path_done) {
-                if (J.chunks > 1) {
+                if (SPLIT || J.chunks > 1) {
                     float* slot = J.lbuf + 3 * ((size_t)pixel * J.sample_count + (sample - J.first_sample));
                     slot[0] = ps.L.x;
                     slot[1] = ps.L.y;
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
                 if (sample < s_end) {
                     new_path(s, J.seed);
                 } else {
-                    if (J.chunks == 1) {
+                    if (!SPLIT && J.chunks == 1) {
                         J.film.rgb[3 * pixel] = acc_r;
                         J.film.rgb[3 * pixel + 1] = acc_g;
                         J.film.rgb[3 * pixel + 2] = acc_b;
@@ -244,7 +246,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
                     const int c = (int)(local / (unsigned)pixels);
                     sample = J.first_sample + c * J.chunk;
                     s_end = min(sample + J.chunk, J.first_sample + J.sample_count);
-                    if (J.chunks == 1) {
+                    if (!SPLIT && J.chunks == 1) {
                         acc_r = J.film.rgb[3 * pixel];
                         acc_g = J.film.rgb[3 * pixel + 1];
                         acc_b = J.film.rgb[3 * pixel + 2];
@@ -322,28 +324,28 @@ __global__ void film_commit_jobs(const JobDesc* jobs, const BatchHeader* hdr) {
         commit_pixel(J.film, J.lbuf, p, J.sample_count);
 }
 
-template <int BLOCK, bool MULTI, int MINB, bool COUNT>
+template <int BLOCK, bool MULTI, int MINB, bool COUNT, bool SPLIT>
 int resident_ctas(int blocks_per_sm) {
     int dev = 0, sms = 0, occ = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_persistent<BLOCK, MULTI, MINB, COUNT>,
-                                                             BLOCK, 0),
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                   &occ, megakernel_persistent<BLOCK, MULTI, MINB, COUNT, SPLIT>, BLOCK, 0),
                "occupancy");
     if (blocks_per_sm > 0 && blocks_per_sm < occ) occ = blocks_per_sm;
     if (occ < 1) occ = 1;
     return sms * occ;
 }
 
-template <int BLOCK, bool MULTI, int MINB, bool COUNT>
+template <int BLOCK, bool MULTI, int MINB, bool COUNT, bool SPLIT>
 void launch_block(const MkArgs& args, long long units, int blocks_per_sm, cudaStream_t stream) {
-    long long grid = resident_ctas<BLOCK, MULTI, MINB, COUNT>(blocks_per_sm);
+    long long grid = resident_ctas<BLOCK, MULTI, MINB, COUNT, SPLIT>(blocks_per_sm);
     if (units > 0) {
         const long long needed = (units + BLOCK - 1) / BLOCK;
         if (grid > needed) grid = needed;
     }
     if (grid < 1) grid = 1;
-    megakernel_persistent<BLOCK, MULTI, MINB, COUNT><<<(unsigned)grid, BLOCK, 0, stream>>>(args);
+    megakernel_persistent<BLOCK, MULTI, MINB, COUNT, SPLIT><<<(unsigned)grid, BLOCK, 0, stream>>>(args);
     cuda_check(cudaGetLastError(), "megakernel launch");
 }
 
@@ -360,15 +362,18 @@ auto dispatch(const MegakernelConfig& cfg, F&& f) {
     return f(std::integral_constant<int, 128>{}, std::integral_constant<int, 1>{});
 }
 
+// `all_split`: every job of the launch has chunks > 1 (selects the SPLIT variant).
 template <bool MULTI>
-void launch_any(const MkArgs& args, long long units, const MegakernelConfig& cfg, cudaStream_t stream) {
-    if (args.count_rays) {  // counting runs use the instrumented 128-thread variant
-        launch_block<128, MULTI, 1, true>(args, units, cfg.blocks_per_sm, stream);
+void launch_any(const MkArgs& args, long long units, const MegakernelConfig& cfg, bool all_split,
+                cudaStream_t stream) {
+    if (args.count_rays) {  // counting runs use the instrumented 128-thread variant (both modes)
+        launch_block<128, MULTI, 1, true, false>(args, units, cfg.blocks_per_sm, stream);
         return;
     }
     dispatch<MULTI>(cfg, [&](auto block, auto minb) {
-        launch_block<decltype(block)::value, MULTI, decltype(minb)::value, false>(args, units, cfg.blocks_per_sm,
-                                                                                  stream);
+        constexpr int B = decltype(block)::value, O = decltype(minb)::value;
+        if (all_split) launch_block<B, MULTI, O, false, true>(args, units, cfg.blocks_per_sm, stream);
+        else launch_block<B, MULTI, O, false, false>(args, units, cfg.blocks_per_sm, stream);
         return 0;
     });
 }
@@ -384,7 +389,7 @@ void launch_film_commit(const DevFilm& film, const float* lbuf, int count, cudaS
 int megakernel_resident_threads(const MegakernelConfig& cfg) {
     return dispatch<false>(cfg, [&](auto block, auto minb) {
         return decltype(block)::value *
-               resident_ctas<decltype(block)::value, false, decltype(minb)::value, false>(cfg.blocks_per_sm);
+               resident_ctas<decltype(block)::value, false, decltype(minb)::value, false, true>(cfg.blocks_per_sm);
     });
 }
 
@@ -432,7 +437,7 @@ int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* count
     args.min_active = cfg.min_active;
     args.leaf_batch = cfg.leaf_batch;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
-    launch_any<false>(args, args.job0.units, cfg, stream);
+    launch_any<false>(args, args.job0.units, cfg, args.job0.chunks > 1, stream);
     if (args.job0.chunks > 1) {
         launch_film_commit(film, lbuf, p.sample_count, stream);
         return 2;
@@ -442,7 +447,7 @@ int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* count
 
 void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, int max_jobs, DevCounters* counters,
                              unsigned int* work_counter, bool count_rays, const MegakernelConfig& cfg,
-                             cudaStream_t stream) {
+                             bool all_split, cudaStream_t stream) {
     MkArgs args{};
     args.jobs = d_jobs;
     args.hdr = d_hdr;
@@ -452,7 +457,7 @@ void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
     args.min_active = cfg.min_active;
     args.leaf_batch = cfg.leaf_batch;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
-    launch_any<true>(args, 0, cfg, stream);  // full persistent grid: the unit count lives on the device
+    launch_any<true>(args, 0, cfg, all_split, stream);  // full persistent grid: the unit count lives on the device
     launch_film_commit_jobs(d_jobs, d_hdr, max_jobs, stream);
 }
 
