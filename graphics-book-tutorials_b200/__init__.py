@@ -444,7 +444,7 @@ class TuneResult:
 def autotune(scene: Scene, width: int, height: int, probe_spp: int = 2, max_depth: int = 8,
              try_wavefront: bool = True) -> TuneResult:
     """Measures launch configurations of both arms on the scene's camera at width x height and returns the
-    fastest; cached per scene hash and size inside the library (wfb_autotune)."""
+    fastest; cached per scene content and size inside the library (wfb_autotune)."""
     c = _CTuneResult()
     _check(load_library().wfb_autotune(scene.handle, int(width), int(height), int(probe_spp), int(max_depth),
                                        1 if try_wavefront else 0, ctypes.byref(c)))

@@ -18,7 +18,7 @@ struct TuneResult {
 };
 
 // Measures candidate configurations of both arms on the scene with camera `cam` at width x height
-// for probe_spp samples and returns the fastest (cached per scene hash and size).
+// for probe_spp samples and returns the fastest (cached per scene content and size).
 TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camera& cam, int width, int height,
                     int probe_spp, int max_depth, bool try_wavefront);
 // Applies the knobs of `t` that belong to the renderer's arm (whichever arm won).

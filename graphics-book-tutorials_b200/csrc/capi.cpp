@@ -5,6 +5,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include "engine.hpp"
 #include "autotune.hpp"
 #include "noalloc.hpp"
@@ -193,9 +194,11 @@ int wfb_scene_create(const wfb_scene_desc* d, int finalize_bins, wfb_scene_t* ou
              "negative array size");
         auto s = std::make_unique<wfb_scene>();
         wf::Scene& h = s->host;
-        auto copy = [](auto& vec, const void* src, int n) {
-            vec.resize((size_t)n);
-            if (n) std::memcpy(vec.data(), src, sizeof(vec[0]) * (size_t)n);
+        auto copy = [](auto& vec, const void* src, int n) {  // one pass: no zero-fill before the copy
+            using T = typename std::decay_t<decltype(vec)>::value_type;
+            const T* p = static_cast<const T*>(src);
+            if (n) vec.assign(p, p + n);
+            else vec.clear();
         };
         need((d->n_spheres == 0 || d->spheres) && (d->n_vertices == 0 || d->vertices) &&
                  (d->n_triangles == 0 || d->triangles) && (d->n_materials == 0 || d->materials) &&

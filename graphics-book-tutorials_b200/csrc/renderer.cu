@@ -9,6 +9,28 @@
 
 namespace wfb {
 
+namespace {
+
+// Film and sample buffers come from the device's stream-ordered pool, which keeps up to this many
+// freed bytes for reuse: creating a renderer per frame (or per scene) then costs no device
+// allocation after the first, where cudaMalloc of a 700 MB sample buffer takes milliseconds.
+constexpr uint64_t kPoolKeepBytes = 8ull << 30;
+
+void keep_pool_memory() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+    uint64_t keep = 0;
+    if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) return;
+    if (keep < kPoolKeepBytes) {
+        keep = kPoolKeepBytes;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+}
+
+}  // namespace
+
 struct Renderer::Wavefront {
     WavefrontConfig cfg;
     WavefrontEngine engine;
@@ -26,6 +48,7 @@ Renderer::Renderer(std::shared_ptr<ResidentScene> scene, wf::GpuMode mode)
     cuda_check(cudaEventCreate(&ev1_), "cudaEventCreate");
     cuda_check(cudaMalloc(&counters_, sizeof(DevCounters)), "cudaMalloc counters");
     cuda_check(cudaMalloc(&work_, 256), "cudaMalloc work counter");
+    keep_pool_memory();
     alloc_film();
 }
 
@@ -34,7 +57,7 @@ Renderer::~Renderer() {
     wf_.reset();
     if (counters_) cudaFree(counters_);
     if (work_) cudaFree(work_);
-    if (lbuf_) cudaFree(lbuf_);
+    if (lbuf_) cudaFreeAsync(lbuf_, stream_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -43,17 +66,18 @@ Renderer::~Renderer() {
 void Renderer::alloc_film() {
     const size_t p = (size_t)width_ * height_;
     float* base = nullptr;
-    cuda_check(cudaMalloc(&base, 5 * p * sizeof(float)), "cudaMalloc film");
+    cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&base), 5 * p * sizeof(float), stream_), "allocate film");
     film_.rgb = base;
     film_.lum = base + 3 * p;
     film_.lum2 = base + 4 * p;
     film_.pixels = (int)p;
-    cuda_check(cudaMemset(base, 0, 5 * p * sizeof(float)), "cudaMemset film");
+    cuda_check(cudaMemsetAsync(base, 0, 5 * p * sizeof(float), stream_), "zero film");
+    cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
     if (mode_ == wf::GpuMode::Wavefront) wf_ = std::make_unique<Wavefront>((int)p, wf_cfg_);
 }
 
 void Renderer::free_film() {
-    if (film_.rgb) cudaFree(film_.rgb);
+    if (film_.rgb) cudaFreeAsync(film_.rgb, stream_);
     film_ = DevFilm{};
     wf_.reset();
 }
@@ -99,10 +123,11 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
             if (chunks > 1) {
                 const size_t need = 3 * (size_t)pixels() * (size_t)q.sample_count;
                 if (need > lbuf_floats_) {
-                    if (lbuf_) cudaFree(lbuf_);
+                    if (lbuf_) cudaFreeAsync(lbuf_, stream_);
                     lbuf_ = nullptr;
                     lbuf_floats_ = 0;
-                    cuda_check(cudaMalloc(&lbuf_, need * sizeof(float)), "cudaMalloc sample buffer");
+                    cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&lbuf_), need * sizeof(float), stream_),
+                               "allocate sample buffer");
                     lbuf_floats_ = need;
                 }
             }

@@ -181,7 +181,7 @@ int wfb_renderer_destroy(wfb_renderer_t r);
  * Measures launch configurations of both arms on `scene` (its camera) at width x height for
  * probe_spp samples: the faster arm (mode), the best megakernel block / occupancy target /
  * min_active / leaf_batch and the best wavefront paths in flight / min_active (0 when the
- * wavefront was not tried). Cached per scene hash and size. */
+ * wavefront was not tried). Cached per scene content and size. */
 typedef struct {
     int mode;
     int block, occupancy, min_active, leaf_batch;
