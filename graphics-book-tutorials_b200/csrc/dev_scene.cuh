@@ -119,31 +119,6 @@ WF_HD wf::LightGeom load_light(const DevScene& s, int idx) {
 }
 
 #if defined(__CUDACC__)
-// Slab test of wf::hit_box without the two early exits: t0 only grows and t1 only shrinks
-// (compare-and-select updates that keep the reference's NaN behaviour), so once t0 > t1 the final
-// t0 <= t1 is false as well -- the result is identical, with fewer branches.
-__device__ __forceinline__ bool hit_box_nobranch(wf::Vec3 lo, wf::Vec3 hi, wf::Vec3 o, wf::Vec3 inv_d, float tmin,
-                                                 float tmax) {
-    float t0 = tmin, t1 = tmax;
-    float tn = (lo.x - o.x) * inv_d.x, tf = (hi.x - o.x) * inv_d.x;
-    float a = tn > tf ? tf : tn, b = tn > tf ? tn : tf;
-    t0 = a > t0 ? a : t0;
-    t1 = b < t1 ? b : t1;
-    tn = (lo.y - o.y) * inv_d.y;
-    tf = (hi.y - o.y) * inv_d.y;
-    a = tn > tf ? tf : tn;
-    b = tn > tf ? tn : tf;
-    t0 = a > t0 ? a : t0;
-    t1 = b < t1 ? b : t1;
-    tn = (lo.z - o.z) * inv_d.z;
-    tf = (hi.z - o.z) * inv_d.z;
-    a = tn > tf ? tf : tn;
-    b = tn > tf ? tn : tf;
-    t0 = a > t0 ? a : t0;
-    t1 = b < t1 ? b : t1;
-    return t0 <= t1;
-}
-
 // Direction of a ray being traversed by the resumable traversal below. Its origin is passed to
 // each step (the path's current ray origin) and its tmin is kRayEps: every ray the estimator
 // creates has tmin = kRayEps (camera_ray, set_next_ray, the shadow ray of shade_lambert,
@@ -172,7 +147,7 @@ __device__ __forceinline__ void box_step(const float4* __restrict__ nodes, int n
     const float4 na = __ldg(&nodes[2 * node]);
     const float4 nb = __ldg(&nodes[2 * node + 1]);
     const int skip = __float_as_int(na.w);
-    if (!hit_box_nobranch(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, o, ray.inv_d, wf::kRayEps, tmax)) {
+    if (!wf::hit_box_minmax(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, o, ray.inv_d, wf::kRayEps, tmax)) {
         node = skip;
     } else {
         const int leaf = __float_as_int(nb.w);

@@ -63,7 +63,7 @@ WF_HD bool hit_triangle(Vec3 p0, Vec3 p1, Vec3 p2, const Ray& r, float* t_out, f
 
 // Slab test on [tmin, tmax]. The compare-and-swap and the two ternary clamps are kept literally:
 // a NaN slab distance (origin on a slab plane with a zero direction component) leaves t0/t1
-// unchanged, which min/max intrinsics would not reproduce.
+// unchanged, which plain min/max would not reproduce (hit_box_minmax maps NaN first).
 WF_HD bool hit_box(Vec3 lo, Vec3 hi, Vec3 o, Vec3 inv_d, float tmin, float tmax) {
     float t0 = tmin, t1 = tmax;
     float tn = (lo.x - o.x) * inv_d.x, tf = (hi.x - o.x) * inv_d.x;
@@ -82,6 +82,26 @@ WF_HD bool hit_box(Vec3 lo, Vec3 hi, Vec3 o, Vec3 inv_d, float tmin, float tmax)
     if (tn > tf) { const float s = tn; tn = tf; tf = s; }
     t0 = tn > t0 ? tn : t0;
     t1 = tf < t1 ? tf : t1;
+    return t0 <= t1;
+}
+
+// hit_box on min/max operations, with the same result for every input, NaN included (the GPU
+// traversal's box test: fminf/fmaxf are one instruction each, a compare-and-select two). In
+// hit_box the early exits and the final t0 <= t1 agree once t0 > t1, so they can go. Per axis, a
+// NaN slab distance (a NaN factor, or 0 * inf when the origin lies on the slab plane of an axis
+// the ray is parallel to) is never swapped, so a NaN tn reaches only the t0 clamp and a NaN tf
+// only the t1 clamp, and a clamp with a NaN operand leaves t0/t1 unchanged. Here a NaN tn reads as
+// -inf and a NaN tf as +inf (fmaxf/fminf return their non-NaN operand), which the clamps ignore in
+// the same way; with no NaN left, compare-and-select and fminf/fmaxf pick the same value up to the
+// sign of a zero, which no comparison sees. t0 starts at tmin, never NaN; a NaN tmax leaves
+// hit_box's t1 NaN and its result false, so tmax joins last, by compare-and-select.
+WF_HD bool hit_box_minmax(Vec3 lo, Vec3 hi, Vec3 o, Vec3 inv_d, float tmin, float tmax) {
+    const float xn = fmaxf((lo.x - o.x) * inv_d.x, -INFINITY), xf = fminf((hi.x - o.x) * inv_d.x, INFINITY);
+    const float yn = fmaxf((lo.y - o.y) * inv_d.y, -INFINITY), yf = fminf((hi.y - o.y) * inv_d.y, INFINITY);
+    const float zn = fmaxf((lo.z - o.z) * inv_d.z, -INFINITY), zf = fminf((hi.z - o.z) * inv_d.z, INFINITY);
+    const float t0 = fmaxf(fmaxf(fminf(xn, xf), fminf(yn, yf)), fmaxf(fminf(zn, zf), tmin));
+    const float b = fminf(fminf(fmaxf(xn, xf), fmaxf(yn, yf)), fmaxf(zn, zf));
+    const float t1 = b < tmax ? b : tmax;
     return t0 <= t1;
 }
 
