@@ -4,7 +4,8 @@
 // Candidates are rendered for `probe_spp` samples at the target resolution, each once to warm up
 // and once timed with CUDA events; the fastest measured configuration wins. Every candidate
 // renders the same film bits (launch knobs never change the arithmetic), so tuning is purely a
-// speed decision. Results are cached per (scene content, width, height, probe_spp, max_depth).
+// speed decision. Results are cached per (scene content, camera, width, height, probe_spp,
+// max_depth); the content key is the uploaded arena's hash (upload_scene).
 // The result holds the best knobs of each arm, so a renderer of either arm can apply it.
 //   megakernel: stage 1, (block, occupancy target) in {(128,10), (128,8), (128,6), (128,0), (64,0), (256,0)}
 //               x min_active in {8, 16, 24} at leaf_batch 8; stage 2, the stage-1 winner with
@@ -27,34 +28,6 @@ using Key = std::tuple<uint64_t, int, int, int, int, bool>;
 std::mutex g_mu;
 std::map<Key, TuneResult> g_cache;
 
-// Cache key of a scene's content: its arrays hashed 8 bytes at a time with a multiply-xorshift
-// mix (about 2.5 ms for 20 MB, where the byte-wise FNV-1a of scene_hash takes about 20 ms). A
-// collision could only reuse launch knobs tuned for another scene -- the film never depends on them.
-uint64_t mix_bytes(uint64_t h, const void* data, size_t bytes) {
-    const unsigned char* p = static_cast<const unsigned char*>(data);
-    size_t i = 0;
-    for (; i + 8 <= bytes; i += 8) {
-        uint64_t w;
-        std::memcpy(&w, p + i, 8);
-        h = (h ^ w) * 0x9E3779B97F4A7C15ull;
-        h ^= h >> 29;
-    }
-    for (; i < bytes; ++i) h = (h ^ p[i]) * 0x100000001B3ull;
-    return h ^ (uint64_t)bytes;
-}
-
-uint64_t content_key(const wf::Scene& s) {
-    uint64_t h = 0x6A09E667F3BCC909ull;
-    h = mix_bytes(h, s.spheres.data(), s.spheres.size() * sizeof(wf::Sphere));
-    h = mix_bytes(h, s.vertices.data(), s.vertices.size() * sizeof(wf::Vec3));
-    h = mix_bytes(h, s.triangles.data(), s.triangles.size() * sizeof(wf::Triangle));
-    h = mix_bytes(h, s.materials.data(), s.materials.size() * sizeof(wf::Material));
-    h = mix_bytes(h, s.nodes.data(), s.nodes.size() * sizeof(wf::BvhNode));
-    h = mix_bytes(h, s.prim_order.data(), s.prim_order.size() * sizeof(int));
-    h = mix_bytes(h, &s.camera, sizeof(s.camera));
-    return mix_bytes(h, &s.env, sizeof(s.env));
-}
-
 double measure(Renderer& r, const PassParams& p) {
     r.reset();
     r.run_passes(p, nullptr);  // warm-up (module load, pool allocation)
@@ -70,7 +43,7 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
                     int probe_spp, int max_depth, bool try_wavefront) {
     if (!scene) throw Error(WFB_ERR_INVALID_ARGUMENT, "null scene");
     if (width <= 0 || height <= 0 || probe_spp <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "bad tuning size");
-    const Key key{content_key(scene->host), width, height, probe_spp, max_depth, try_wavefront};
+    const Key key{mix_key(scene->content_key, &cam, sizeof(cam)), width, height, probe_spp, max_depth, try_wavefront};
     {
         std::lock_guard<std::mutex> lock(g_mu);
         auto it = g_cache.find(key);

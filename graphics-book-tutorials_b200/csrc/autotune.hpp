@@ -8,7 +8,7 @@ namespace wfb {
 struct TuneResult {
     int mode = 0;  // the faster arm: WFB_MODE_MEGAKERNEL or WFB_MODE_WAVEFRONT
     // Best megakernel knobs.
-    int block = 128, occupancy = 0, min_active = 24, leaf_batch = 8;
+    int block = 128, occupancy = 0, min_active = 16, leaf_batch = 8;
     // Best wavefront knobs (0: not tried, library defaults).
     int paths_in_flight = 0, wf_min_active = 0;
     double msamples_s = 0.0;             // the winner's measured rate

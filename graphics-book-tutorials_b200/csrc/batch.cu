@@ -13,30 +13,6 @@
 
 namespace wfb {
 
-void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream) {
-    if (spp_done <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "spp_done must be positive");
-    const size_t p = (size_t)film.pixels;
-    std::vector<float> lum, lum2;
-    if (stream) cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
-    if (rgb) cuda_check(cudaMemcpy(rgb, film.rgb, 3 * p * sizeof(float), cudaMemcpyDeviceToHost), "download rgb");
-    if (lum_var) {
-        lum.resize(p);
-        lum2.resize(p);
-        cuda_check(cudaMemcpy(lum.data(), film.lum, p * sizeof(float), cudaMemcpyDeviceToHost), "download lum");
-        cuda_check(cudaMemcpy(lum2.data(), film.lum2, p * sizeof(float), cudaMemcpyDeviceToHost), "download lum2");
-    }
-    // GPU-arm convention (WVM/src/gpu/gpu_renderer.cu:319-338): float reciprocal, double variance.
-    const float inv = 1.0f / (float)spp_done;
-    if (rgb)
-        for (size_t i = 0; i < 3 * p; ++i) rgb[i] *= inv;
-    if (lum_var)
-        for (size_t i = 0; i < p; ++i) {
-            const double m = (double)lum[i] / (double)spp_done;
-            const double m2 = (double)lum2[i] / (double)spp_done;
-            lum_var[i] = (float)std::max(0.0, m2 - m * m);
-        }
-}
-
 // ---------------------------------------------------------------------------------------------
 BatchLauncher::BatchLauncher(int max_jobs, const LaunchConfig& cfg) : max_jobs_(max_jobs), cfg_(cfg) {
     if (max_jobs <= 0 || max_jobs > 65535) throw Error(WFB_ERR_INVALID_ARGUMENT, "max_jobs must be in 1..65535");

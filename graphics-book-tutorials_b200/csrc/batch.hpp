@@ -96,8 +96,5 @@ private:
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 };
 
-// Host-side conversions shared by renderers, batches and the server. `stream` is synchronised
-// first unless it is null (the caller has already waited for the work that wrote the film).
-void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream);
 
 }  // namespace wfb

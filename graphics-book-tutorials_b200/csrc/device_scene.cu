@@ -2,6 +2,7 @@
 // Host arithmetic in this file is compiled without contraction (-ffp-contract=off) so every
 // precomputed float equals the one the reference computes per ray.
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "engine.hpp"
@@ -48,7 +49,58 @@ DevScene with_camera(const DevScene& s, const wf::Camera& cam, int width, int he
     return v;
 }
 
-std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
+namespace {
+
+// Pinned host staging for scene uploads, reused by every upload of the process (grown when a
+// larger scene arrives, never returned): the packed arrays are written straight into it and cross
+// PCIe in one copy, instead of being built in fresh pageable vectors (page faults) and copied by
+// the driver through its own bounce buffer.
+struct Staging {
+    std::mutex mu;
+    char* p = nullptr;
+    size_t cap = 0;
+};
+Staging& staging() {
+    static Staging* s = new Staging;  // not freed at exit: the CUDA runtime may be gone by then
+    return *s;
+}
+
+// Cache key of a packed arena: 4 KB chunks hashed on the device 8 bytes at a time with a
+// multiply-xorshift mix; the host folds the chunk hashes in order.
+constexpr size_t kHashChunkWords = 512;
+__global__ void hash_chunks(const unsigned long long* __restrict__ w, size_t n_words, unsigned long long* out) {
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t begin = c * kHashChunkWords;
+    if (begin >= n_words) return;
+    const size_t end = begin + kHashChunkWords < n_words ? begin + kHashChunkWords : n_words;
+    unsigned long long h = 0x6A09E667F3BCC909ull ^ c;
+    for (size_t i = begin; i < end; ++i) {
+        h = (h ^ w[i]) * 0x9E3779B97F4A7C15ull;
+        h ^= h >> 29;
+    }
+    out[c] = h;
+}
+
+uint64_t fold(uint64_t h, uint64_t w) {
+    h = (h ^ w) * 0x9E3779B97F4A7C15ull;
+    return h ^ (h >> 29);
+}
+
+}  // namespace
+
+uint64_t mix_key(uint64_t h, const void* data, size_t bytes) {
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    size_t i = 0;
+    for (; i + 8 <= bytes; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, p + i, 8);
+        h = fold(h, w);
+    }
+    for (; i < bytes; ++i) h = (h ^ p[i]) * 0x100000001B3ull;
+    return h ^ (uint64_t)bytes;
+}
+
+std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
     if (host.nodes.empty()) throw Error(WFB_ERR_NOT_FINALIZED, "Scene not finalized (no BVH nodes)");
     if (host.width <= 0 || host.height <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "scene resolution must be positive");
     if (host.materials.empty()) throw Error(WFB_ERR_INVALID_ARGUMENT, "no materials");
@@ -68,8 +120,45 @@ std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
             throw Error(WFB_ERR_INVALID_ARGUMENT, "triangle vertex index out of range");
     }
 
+    // One arena of 256-byte aligned parts, packed in pinned staging and copied once.
+    enum { kNodes, kPrims, kSpheres, kTriShade, kTriArea, kMaterials, kLights, kParts };
+    const size_t bytes[kParts] = {(size_t)2 * nn * 16,          (size_t)3 * (np > 0 ? np : 1) * 16,
+                                  (size_t)2 * (ns > 0 ? ns : 1) * 16, (size_t)(nt > 0 ? nt : 1) * 16,
+                                  (size_t)(nt > 0 ? nt : 1) * 4,  (size_t)nm * sizeof(wf::Material),
+                                  (size_t)4 * (nl > 0 ? nl : 1) * 16};
+    size_t off[kParts], total = 0;
+    for (int k = 0; k < kParts; ++k) {
+        off[k] = total;
+        total += align256(bytes[k]);
+    }
+    Staging& st = staging();
+    std::lock_guard<std::mutex> lock(st.mu);
+    if (st.cap < total) {
+        if (st.p) cuda_check(cudaFreeHost(st.p), "cudaFreeHost staging");
+        st.p = nullptr;
+        st.cap = 0;
+        const size_t cap = (total + (16u << 20) - 1) & ~(size_t)((16u << 20) - 1);
+        cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&st.p), cap, cudaHostAllocPortable), "cudaHostAlloc staging");
+        st.cap = cap;
+    }
+    char* stage = st.p;
+    // Padding, placeholder records of empty parts and unused words are zero, so the arena (and its
+    // hash) depends on the scene only.
+    for (int k = 0; k < kParts; ++k) std::memset(stage + off[k] + bytes[k], 0, align256(bytes[k]) - bytes[k]);
+    if (np == 0) std::memset(stage + off[kPrims], 0, bytes[kPrims]);
+    if (ns == 0) std::memset(stage + off[kSpheres], 0, bytes[kSpheres]);
+    if (nt == 0) {
+        std::memset(stage + off[kTriShade], 0, bytes[kTriShade]);
+        std::memset(stage + off[kTriArea], 0, bytes[kTriArea]);
+    }
+    if (nl == 0) std::memset(stage + off[kLights], 0, bytes[kLights]);
+    float4* nodes = reinterpret_cast<float4*>(stage + off[kNodes]);
+    float4* prims = reinterpret_cast<float4*>(stage + off[kPrims]);
+    float4* tri_shade = reinterpret_cast<float4*>(stage + off[kTriShade]);
+    float* tri_area = reinterpret_cast<float*>(stage + off[kTriArea]);
+    float4* lights = reinterpret_cast<float4*>(stage + off[kLights]);
+
     // Nodes: {lo, skip} {hi, leaf}.
-    std::vector<float4> nodes((size_t)2 * nn);
     for (int i = 0; i < nn; ++i) {
         const wf::BvhNode& n = host.nodes[i];
         int leaf = -1;
@@ -88,7 +177,6 @@ std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
         nodes[2 * i + 1] = f4(n.hi, i2f(leaf));
     }
     // Leaf primitive records in prim_order order.
-    std::vector<float4> prims((size_t)3 * (np > 0 ? np : 1), make_float4(0, 0, 0, 0));
     for (int j = 0; j < np; ++j) {
         const int p = host.prim_order[j];
         if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "prim_order entry out of range");
@@ -96,6 +184,7 @@ std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
             const wf::Sphere& s = host.spheres[p];
             prims[3 * j] = f4(s.center, i2f(p));
             prims[3 * j + 1] = make_float4(s.radius, 0, 0, 0);
+            prims[3 * j + 2] = make_float4(0, 0, 0, 0);
         } else {
             const wf::Triangle& t = host.triangles[p - ns];
             const wf::Vec3 p0 = host.vertices[t.i0];
@@ -105,10 +194,7 @@ std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
         }
     }
     // Spheres (wf::Sphere bytes), triangle shading records and areas, materials.
-    std::vector<float4> spheres((size_t)2 * (ns > 0 ? ns : 1), make_float4(0, 0, 0, 0));
-    if (ns) std::memcpy(spheres.data(), host.spheres.data(), sizeof(wf::Sphere) * ns);
-    std::vector<float4> tri_shade(nt > 0 ? nt : 1, make_float4(0, 0, 0, 0));
-    std::vector<float> tri_area(nt > 0 ? nt : 1, 0.0f);
+    if (ns) std::memcpy(stage + off[kSpheres], host.spheres.data(), sizeof(wf::Sphere) * ns);
     for (int i = 0; i < nt; ++i) {
         const wf::Triangle& t = host.triangles[i];
         const wf::Vec3 e1 = host.vertices[t.i1] - host.vertices[t.i0];
@@ -116,10 +202,8 @@ std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
         tri_shade[i] = f4(wf::normalize(wf::cross(e1, e2)), i2f(t.material));
         tri_area[i] = 0.5f * wf::length(wf::cross(e1, e2));
     }
-    std::vector<float4> materials((size_t)3 * nm);
-    std::memcpy(materials.data(), host.materials.data(), sizeof(wf::Material) * nm);
+    std::memcpy(stage + off[kMaterials], host.materials.data(), sizeof(wf::Material) * nm);
     // Lights: {a, prim} {b, area} {c, material} {n, radius}.
-    std::vector<float4> lights((size_t)4 * (nl > 0 ? nl : 1), make_float4(0, 0, 0, 0));
     for (int i = 0; i < nl; ++i) {
         const int p = host.lights[i].prim;
         if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "light primitive out of range");
@@ -141,36 +225,33 @@ std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
         }
     }
 
-    // One arena, 256-byte aligned sub-buffers.
-    struct Part {
-        const void* src;
-        size_t bytes;
-        size_t off;
-    };
-    Part parts[] = {{nodes.data(), nodes.size() * 16, 0},       {prims.data(), prims.size() * 16, 0},
-                    {spheres.data(), spheres.size() * 16, 0},   {tri_shade.data(), tri_shade.size() * 16, 0},
-                    {tri_area.data(), tri_area.size() * 4, 0},  {materials.data(), materials.size() * 16, 0},
-                    {lights.data(), lights.size() * 16, 0}};
-    size_t total = 0;
-    for (Part& p : parts) {
-        p.off = total;
-        total += align256(p.bytes);
-    }
     auto rs = std::make_shared<ResidentScene>();
     cuda_check(cudaGetDevice(&rs->device), "cudaGetDevice");
-    cuda_check(cudaMalloc(&rs->arena, total), "cudaMalloc scene");
+    const size_t n_chunks = (total / 8 + kHashChunkWords - 1) / kHashChunkWords;
+    cuda_check(cudaMalloc(&rs->arena, total + n_chunks * 8), "cudaMalloc scene");
     rs->bytes = total;
     char* base = static_cast<char*>(rs->arena);
-    for (const Part& p : parts)
-        cuda_check(cudaMemcpy(base + p.off, p.src, p.bytes, cudaMemcpyHostToDevice), "cudaMemcpy scene");
+    cuda_check(cudaMemcpy(base, stage, total, cudaMemcpyHostToDevice), "cudaMemcpy scene");
+    // Content key: chunk hashes of the arena (in the tail of the same allocation), folded here.
+    unsigned long long* chunk_hash = reinterpret_cast<unsigned long long*>(base + total);
+    hash_chunks<<<(unsigned)((n_chunks + 255) / 256), 256>>>(reinterpret_cast<const unsigned long long*>(base),
+                                                              total / 8, chunk_hash);
+    cuda_check(cudaGetLastError(), "hash_chunks launch");
+    std::vector<unsigned long long> hashes(n_chunks);
+    cuda_check(cudaMemcpy(hashes.data(), chunk_hash, n_chunks * 8, cudaMemcpyDeviceToHost), "cudaMemcpy hashes");
+    uint64_t key = 0x6A09E667F3BCC909ull ^ total;
+    for (unsigned long long h : hashes) key = fold(key, h);
+    key = mix_key(key, &host.env, sizeof(host.env));
+    rs->content_key = mix_key(key, &host.camera, sizeof(host.camera));
+
     DevScene& d = rs->dev;
-    d.nodes = reinterpret_cast<const float4*>(base + parts[0].off);
-    d.prims = reinterpret_cast<const float4*>(base + parts[1].off);
-    d.spheres = reinterpret_cast<const float4*>(base + parts[2].off);
-    d.tri_shade = reinterpret_cast<const float4*>(base + parts[3].off);
-    d.tri_area = reinterpret_cast<const float*>(base + parts[4].off);
-    d.materials = reinterpret_cast<const float4*>(base + parts[5].off);
-    d.lights = reinterpret_cast<const float4*>(base + parts[6].off);
+    d.nodes = reinterpret_cast<const float4*>(base + off[kNodes]);
+    d.prims = reinterpret_cast<const float4*>(base + off[kPrims]);
+    d.spheres = reinterpret_cast<const float4*>(base + off[kSpheres]);
+    d.tri_shade = reinterpret_cast<const float4*>(base + off[kTriShade]);
+    d.tri_area = reinterpret_cast<const float*>(base + off[kTriArea]);
+    d.materials = reinterpret_cast<const float4*>(base + off[kMaterials]);
+    d.lights = reinterpret_cast<const float4*>(base + off[kLights]);
     d.n_spheres = ns;
     d.n_triangles = nt;
     d.n_materials = nm;
@@ -180,7 +261,6 @@ std::shared_ptr<ResidentScene> upload_scene(wf::Scene host) {
     d.camera = wf::make_camera_rig(host.camera, host.width, host.height);
     d.width = host.width;
     d.height = host.height;
-    rs->host = std::move(host);
     return rs;
 }
 

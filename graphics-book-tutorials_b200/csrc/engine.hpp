@@ -23,16 +23,25 @@ void cuda_check(cudaError_t e, const char* what);  // throws Error(WFB_ERR_CUDA 
 // Scene uploaded once in the packed device layout; shared (reference-counted) by every renderer
 // and batch job that draws it, so a BVH stays resident across renders.
 struct ResidentScene {
-    wf::Scene host;  // finalized host copy (source of truth for export, hashing, cameras)
     DevScene dev{};  // device pointers into `arena`; camera/resolution are the host defaults
     void* arena = nullptr;
     uint64_t bytes = 0;
+    uint64_t content_key = 0;   // hash of the packed arena, environment and default camera
     int device = -1;
     ~ResidentScene();
 };
 
 // Validates and repacks a finalized scene into the device layout (see dev_scene.cuh).
-std::shared_ptr<ResidentScene> upload_scene(wf::Scene host);
+std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host);
+
+// Folds `bytes` of `data` into the key `h` (multiply-xorshift over 8-byte words).
+uint64_t mix_key(uint64_t h, const void* data, size_t bytes);
+
+// Film download in the GPU-arm convention (mean rgb, luminance variance), resolved on the device;
+// shared by renderers, batches and the server. Ordered after the work already queued on `stream`
+// (null: the calling thread's own stream, for a film whose writers have finished); returns once
+// the host buffers hold the result. rgb or lum_var may be null.
+void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream);
 
 // Same scene view with another camera / resolution (batch jobs and orbit cameras).
 DevScene with_camera(const DevScene& s, const wf::Camera& cam, int width, int height);
@@ -52,7 +61,7 @@ struct PassParams {
 struct MegakernelConfig {
     int block = 128;        // threads per CTA (64, 128 or 256)
     int blocks_per_sm = 0;  // 0: as many as fit
-    int min_active = 24;    // traverse on while at least this many lanes of a warp traverse
+    int min_active = 16;    // traverse on while at least this many lanes of a warp traverse
     int split_chunks = 0;   // work units per pixel; 0: one sample per unit while its buffer fits
     int occupancy = 10;     // block 128 only: 6, 8 or 10 caps registers for that many CTAs per SM (0: none)
     int leaf_batch = 8;     // a warp tests primitives once this many lanes hold a pending leaf

@@ -29,6 +29,28 @@ void keep_pool_memory() {
     }
 }
 
+// Reference download convention on the device (WVM/src/gpu/gpu_renderer.cu:306-337): mean rgb =
+// sum * (1 / spp) in float; luminance variance = max(0, E[l^2] - E[l]^2) in double, narrowed to
+// float. The same IEEE operations in the same order as the reference's host loops (this file is
+// built without contraction), so the downloaded films are bit-identical; only the resolved film
+// crosses PCIe.
+__global__ void film_resolve(DevFilm film, int spp, float* __restrict__ rgb, float* __restrict__ lum_var) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= film.pixels) return;
+    if (rgb) {
+        const float inv = 1.0f / (float)spp;
+        rgb[3 * p] = film.rgb[3 * p] * inv;
+        rgb[3 * p + 1] = film.rgb[3 * p + 1] * inv;
+        rgb[3 * p + 2] = film.rgb[3 * p + 2] * inv;
+    }
+    if (lum_var) {
+        const double m = (double)film.lum[p] / (double)spp;
+        const double m2 = (double)film.lum2[p] / (double)spp;
+        const double var = m2 - m * m;
+        lum_var[p] = (float)(0.0 < var ? var : 0.0);  // std::max(0.0, var)
+    }
+}
+
 }  // namespace
 
 struct Renderer::Wavefront {
@@ -105,32 +127,38 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
     if (p.sample_count < 0 || p.first_sample < 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "negative sample range");
     if (p.max_depth < 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "max_depth must be >= 0");
     cuda_check(cudaMemsetAsync(counters_, 0, sizeof(DevCounters), stream_), "zero counters");
-    cuda_check(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    // Automatic splitting: a megakernel render whose per-sample buffer would pass the cap runs as
+    // consecutive sub-passes of sample ranges; each pixel still gets its samples in ascending order,
+    // so the film is the same. The sample buffer is sized for the largest sub-pass before the
+    // timed region starts.
+    int step = p.sample_count;
     if (mode_ == wf::GpuMode::Megakernel) {
-        // Automatic splitting: a render whose per-sample buffer would pass the cap runs as
-        // consecutive sub-passes of sample ranges; each pixel still gets its samples in ascending
-        // order, so the film is the same.
-        int step = p.sample_count;
         if (mk_cfg_.split_chunks == 0 && p.sample_count > 1 &&
             split_buffer_bytes(pixels(), p.sample_count) > kSplitBufferBytes)
             step = (int)std::max<uint64_t>(1, kSplitBufferBytes / split_buffer_bytes(pixels(), 1));
+        const int first = std::min(step, p.sample_count);
+        if (first > 0 && megakernel_split_chunks(pixels(), first, mk_cfg_) > 1) {
+            const size_t need = 3 * (size_t)pixels() * (size_t)first;
+            if (need > lbuf_floats_) {
+                if (lbuf_) cudaFreeAsync(lbuf_, stream_);
+                lbuf_ = nullptr;
+                lbuf_floats_ = 0;
+                cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&lbuf_), need * sizeof(float), stream_),
+                           "allocate sample buffer");
+                lbuf_floats_ = need;
+            }
+        }
+    }
+    cuda_check(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
+    if (mode_ == wf::GpuMode::Megakernel) {
         last_launches_ = 0;
         for (int done = 0; done < p.sample_count; done += step) {
             PassParams q = p;
             q.first_sample = p.first_sample + done;
             q.sample_count = std::min(step, p.sample_count - done);
             const int chunks = megakernel_split_chunks(pixels(), q.sample_count, mk_cfg_);
-            if (chunks > 1) {
-                const size_t need = 3 * (size_t)pixels() * (size_t)q.sample_count;
-                if (need > lbuf_floats_) {
-                    if (lbuf_) cudaFreeAsync(lbuf_, stream_);
-                    lbuf_ = nullptr;
-                    lbuf_floats_ = 0;
-                    cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&lbuf_), need * sizeof(float), stream_),
-                               "allocate sample buffer");
-                    lbuf_floats_ = need;
-                }
-            }
+            if (chunks > 1 && 3 * (size_t)pixels() * (size_t)q.sample_count > lbuf_floats_)
+                throw Error(WFB_ERR_INTERNAL, "sample buffer smaller than a sub-pass");
             last_launches_ += launch_megakernel(view_, film_, counters_, work_, lbuf_, q, mk_cfg_, chunks, stream_);
         }
     } else {
@@ -166,26 +194,28 @@ void Renderer::download_sums(float* rgb_sum, float* lum_sum, float* lum2_sum) {
     if (lum2_sum) cuda_check(cudaMemcpy(lum2_sum, film_.lum2, p * sizeof(float), cudaMemcpyDeviceToHost), "download lum2");
 }
 
-void Renderer::download(int spp_done, float* rgb, float* lum_var) {
+void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream) {
     if (spp_done <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "spp_done must be positive");
-    const size_t p = (size_t)pixels();
-    std::vector<float> lum, lum2;
-    if (lum_var) {
-        lum.resize(p);
-        lum2.resize(p);
-    }
-    download_sums(rgb, lum_var ? lum.data() : nullptr, lum_var ? lum2.data() : nullptr);
-    const float inv = 1.0f / (float)spp_done;
-    if (rgb)
-        for (size_t i = 0; i < 3 * p; ++i) rgb[i] *= inv;
-    if (lum_var) {
-        for (size_t i = 0; i < p; ++i) {
-            const double m = (double)lum[i] / (double)spp_done;
-            const double m2 = (double)lum2[i] / (double)spp_done;
-            lum_var[i] = (float)std::max(0.0, m2 - m * m);
-        }
-    }
+    if (!rgb && !lum_var) return;
+    const cudaStream_t s = stream ? stream : cudaStreamPerThread;
+    const size_t p = (size_t)film.pixels;
+    float* out = nullptr;
+    cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&out), 4 * p * sizeof(float), s), "allocate download");
+    (void)cudaGetLastError();  // the check below is for this launch only, not an earlier unchecked call
+    film_resolve<<<(unsigned)((p + 255) / 256), 256, 0, s>>>(film, spp_done, rgb ? out : nullptr,
+                                                              lum_var ? out + 3 * p : nullptr);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && rgb) e = cudaMemcpyAsync(rgb, out, 3 * p * sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && lum_var)
+        e = cudaMemcpyAsync(lum_var, out + 3 * p, p * sizeof(float), cudaMemcpyDeviceToHost, s);
+    const cudaError_t ef = cudaFreeAsync(out, s);
+    const cudaError_t es = cudaStreamSynchronize(s);
+    cuda_check(e, "download film");
+    cuda_check(ef, "free download");
+    cuda_check(es, "cudaStreamSynchronize");
 }
+
+void Renderer::download(int spp_done, float* rgb, float* lum_var) { film_download(film_, spp_done, rgb, lum_var, stream_); }
 
 void Renderer::download_mean(int spp_done, float* rgb) { download(spp_done, rgb, nullptr); }
 

@@ -84,6 +84,8 @@ void Server::shutdown() {
             cudaFreeAsync(kv.second->mem, stream_);
             kv.second->mem = nullptr;
         }
+    for (void* m : to_free_) cudaFreeAsync(m, stream_);
+    to_free_.clear();
     if (stream_) {
         cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
@@ -396,13 +398,15 @@ void Server::worker() {
 // The film is final: its job's last launch has finished and no later launch renders it.
 void Server::downloader() {
     cudaSetDevice(device_);
+    cudaStream_t dl_stream = nullptr;  // this thread's copies: ordered after nothing but themselves
+    const cudaError_t se = cudaStreamCreateWithFlags(&dl_stream, cudaStreamNonBlocking);
     for (;;) {
         uint64_t ticket;
         Job* j;
         {
             std::unique_lock<std::mutex> lock(mu_);
             cv_dl_.wait(lock, [&] { return stop_ || !dl_queue_.empty(); });
-            if (dl_queue_.empty()) return;  // stopping with nothing left to copy
+            if (dl_queue_.empty()) break;  // stopping with nothing left to copy
             ticket = dl_queue_.front();
             dl_queue_.pop_front();
             j = jobs_[ticket].get();
@@ -412,7 +416,8 @@ void Server::downloader() {
         try {
             j->rgb.resize(3 * p);
             j->lum_var.resize(p);
-            film_download(j->buf.film, j->spec.sample_count, j->rgb.data(), j->lum_var.data(), nullptr);
+            cuda_check(se, "cudaStreamCreate download");
+            film_download(j->buf.film, j->spec.sample_count, j->rgb.data(), j->lum_var.data(), dl_stream);
         } catch (const std::exception& e) {
             err = e.what();
         }
@@ -431,28 +436,34 @@ void Server::downloader() {
                     st_.failed++;
                 }
             }
-            release_idle_locked();  // frees the film's device memory (and forgets a cancelled job)
+            release_idle_locked(false);  // the worker frees the film's memory (stream_ is its own)
         }
         cv_done_.notify_all();
         cv_work_.notify_one();  // memory came back: more jobs may be admitted
     }
+    if (dl_stream) cudaStreamDestroy(dl_stream);
 }
 
-// Frees the device memory of jobs that left the active set (done, failed or cancelled) once no
-// launch in flight renders them; cancelled jobs are forgotten, finished ones wait for result().
-void Server::release_idle_locked() {
+// Releases jobs that left the active set (done, failed or cancelled) once no launch in flight
+// renders them; cancelled jobs are forgotten, finished ones wait for result(). Their device memory
+// is freed on stream_ by the worker, the only thread that enqueues work there (it may be capturing
+// a graph on it); other threads leave it in to_free_ for the worker's next call.
+void Server::release_idle_locked(bool worker) {
     for (auto it = active_.begin(); it != active_.end();) {
         Job& j = *jobs_[*it];
         if (j.state == kActive || j.inflight > 0 || j.downloading) {
             ++it;
             continue;
         }
-        if (j.mem) cudaFreeAsync(j.mem, stream_);
+        if (j.mem) to_free_.push_back(j.mem);
         j.mem = nullptr;
         bytes_in_use_ -= j.bytes;
         if (j.state == kCancelled) jobs_.erase(*it);
         it = active_.erase(it);
     }
+    if (!worker) return;
+    for (void* m : to_free_) cudaFreeAsync(m, stream_);
+    to_free_.clear();
 }
 
 }  // namespace wfb

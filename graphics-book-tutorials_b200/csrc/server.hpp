@@ -62,7 +62,7 @@ private:
     void worker();
     uint64_t job_bytes(const Job& j) const;
     bool admit_locked();
-    void release_idle_locked();
+    void release_idle_locked(bool worker = true);
     void downloader();
     int choose_slice(const std::vector<Job*>& act);
 
@@ -82,6 +82,7 @@ private:
     std::thread dl_thread_;               // copies finished films to the host
     std::condition_variable cv_dl_;
     std::deque<uint64_t> dl_queue_;
+    std::vector<void*> to_free_;          // device memory released off the worker, freed by it
     uint64_t bytes_in_use_ = 0, peak_bytes_ = 0;
     double msps_estimate_ = 500.0;  // Msamples/s, refined by launches that filled their budget
     std::vector<double> latencies_ms_;

@@ -142,6 +142,44 @@ def test_served_jobs_equal_solo_renders(wfb, scenes, kw):
     srv.close()
 
 
+def test_results_collected_while_the_server_keeps_launching(wfb, scenes):
+    """A collector takes each result as soon as its job is done while later jobs still arrive and
+    launch (graph replay): finished jobs leave the server while their films' memory is still to be
+    freed by the worker, and every job completes with its solo render's film."""
+    jobs = small_jobs(wfb, scenes, 48, seed=23)
+    srv = wfb.Server(launch_target_ms=2.0)
+    tickets, got, errors = [], {}, []
+    ready = threading.Condition()
+
+    def collector():
+        for k in range(len(jobs)):
+            with ready:
+                ready.wait_for(lambda: len(tickets) > k)
+                t = tickets[k]
+            try:
+                assert srv.wait(t, 60000)
+                got[k] = srv.result(t)[0]
+            except Exception as e:  # surfaced below
+                errors.append((k, repr(e)))
+
+    th = threading.Thread(target=collector)
+    th.start()
+    for s, j in jobs:
+        t = srv.submit(s, j)
+        with ready:
+            tickets.append(t)
+            ready.notify_all()
+        time.sleep(0.003)
+    th.join()
+    assert errors == []
+    for k in (0, 1, 17, 47):
+        s, j = jobs[k]
+        assert np.array_equal(bits(got[k].rgb), bits(solo(wfb, s, j).rgb))
+    st = srv.stats()
+    assert st["completed"] == len(jobs) and st["failed"] == 0
+    srv.close()
+
+
 def test_server_budget_cancel_and_concurrent_submitters(wfb, scenes):
     s = scenes["icospheres"]
     job = wfb.JobDesc(cam_position=(0.0, 6.0, 17.0), cam_look_at=(0.0, 0.5, 0.0), width=128, height=72, spp=8,
