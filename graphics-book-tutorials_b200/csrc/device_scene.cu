@@ -2,7 +2,11 @@
 // Host arithmetic in this file is compiled without contraction (-ffp-contract=off) so every
 // precomputed float equals the one the reference computes per ray.
 #include <cstring>
+#include <exception>
+#include <functional>
+#include <initializer_list>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 #include "engine.hpp"
@@ -22,7 +26,9 @@ ResidentScene::~ResidentScene() {
         int cur = -1;
         cudaGetDevice(&cur);
         if (device >= 0 && cur != device) cudaSetDevice(device);
-        cudaFree(arena);
+        // No kernel reads the scene any more: every render and batch launch waits for its kernels
+        // before returning, and renderers and batches hold the scene while they exist.
+        cudaFreeAsync(arena, 0);
         if (device >= 0 && cur != device && cur >= 0) cudaSetDevice(cur);
     }
 }
@@ -84,6 +90,34 @@ __global__ void hash_chunks(const unsigned long long* __restrict__ w, size_t n_w
 uint64_t fold(uint64_t h, uint64_t w) {
     h = (h ^ w) * 0x9E3779B97F4A7C15ull;
     return h ^ (h >> 29);
+}
+
+// Runs the sections in order, or each on its own thread when `parallel`; rethrows the error of the
+// first section (in order) that failed.
+void run_sections(std::initializer_list<std::function<void()>> sections, bool parallel) {
+    if (!parallel) {
+        for (const auto& f : sections) f();
+        return;
+    }
+    const std::vector<std::function<void()>> fs(sections);
+    std::vector<std::exception_ptr> errs(fs.size());
+    std::vector<std::thread> threads;
+    for (size_t k = 1; k < fs.size(); ++k)
+        threads.emplace_back([&, k] {
+            try {
+                fs[k]();
+            } catch (...) {
+                errs[k] = std::current_exception();
+            }
+        });
+    try {
+        fs[0]();
+    } catch (...) {
+        errs[0] = std::current_exception();
+    }
+    for (auto& t : threads) t.join();
+    for (const auto& e : errs)
+        if (e) std::rethrow_exception(e);
 }
 
 }  // namespace
@@ -158,84 +192,99 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
     float* tri_area = reinterpret_cast<float*>(stage + off[kTriArea]);
     float4* lights = reinterpret_cast<float4*>(stage + off[kLights]);
 
-    // Nodes: {lo, skip} {hi, leaf}.
-    for (int i = 0; i < nn; ++i) {
-        const wf::BvhNode& n = host.nodes[i];
-        int leaf = -1;
-        if (n.prim_count > 0) {
-            if (n.prim_count > kMaxLeafPrims)
-                throw Error(WFB_ERR_UNSUPPORTED, "BVH leaf holds more than 15 primitives");
-            if (n.prim_start < 0 || (long long)n.prim_start + n.prim_count > np || n.prim_start > kMaxLeafStart)
-                throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH leaf prim_start/count out of bounds");
-            leaf = (n.prim_start << kLeafCountBits) | n.prim_count;
+    // The four parts are packed on their own threads for large scenes; an error is reported from
+    // the first part (in this order) that found one, as a serial pass would.
+    auto pack_nodes = [&] {
+        // Nodes: {lo, skip} {hi, leaf}.
+        for (int i = 0; i < nn; ++i) {
+            const wf::BvhNode& n = host.nodes[i];
+            int leaf = -1;
+            if (n.prim_count > 0) {
+                if (n.prim_count > kMaxLeafPrims)
+                    throw Error(WFB_ERR_UNSUPPORTED, "BVH leaf holds more than 15 primitives");
+                if (n.prim_start < 0 || (long long)n.prim_start + n.prim_count > np || n.prim_start > kMaxLeafStart)
+                    throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH leaf prim_start/count out of bounds");
+                leaf = (n.prim_start << kLeafCountBits) | n.prim_count;
+            }
+            if (n.skip < -1 || n.skip >= nn) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link out of bounds");
+            // Every traversal step moves forward (to N+1 or to a forward skip), so a traversal ends
+            // after at most n_nodes steps; a backward skip could loop forever and is rejected.
+            if (n.skip != -1 && n.skip <= i) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link does not point forward");
+            nodes[2 * i] = f4(n.lo, i2f(n.skip));
+            nodes[2 * i + 1] = f4(n.hi, i2f(leaf));
         }
-        if (n.skip < -1 || n.skip >= nn) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link out of bounds");
-        // Every traversal step moves forward (to N+1 or to a forward skip), so a traversal ends
-        // after at most n_nodes steps; a backward skip could loop forever and is rejected.
-        if (n.skip != -1 && n.skip <= i) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link does not point forward");
-        nodes[2 * i] = f4(n.lo, i2f(n.skip));
-        nodes[2 * i + 1] = f4(n.hi, i2f(leaf));
-    }
-    // Leaf primitive records in prim_order order.
-    for (int j = 0; j < np; ++j) {
-        const int p = host.prim_order[j];
-        if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "prim_order entry out of range");
-        if (p < ns) {
-            const wf::Sphere& s = host.spheres[p];
-            prims[3 * j] = f4(s.center, i2f(p));
-            prims[3 * j + 1] = make_float4(s.radius, 0, 0, 0);
-            prims[3 * j + 2] = make_float4(0, 0, 0, 0);
-        } else {
-            const wf::Triangle& t = host.triangles[p - ns];
-            const wf::Vec3 p0 = host.vertices[t.i0];
-            prims[3 * j] = f4(p0, i2f(p));
-            prims[3 * j + 1] = f4(host.vertices[t.i1] - p0, 0.0f);
-            prims[3 * j + 2] = f4(host.vertices[t.i2] - p0, 0.0f);
+    };
+    auto pack_prims = [&] {
+        // Leaf primitive records in prim_order order.
+        for (int j = 0; j < np; ++j) {
+            const int p = host.prim_order[j];
+            if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "prim_order entry out of range");
+            if (p < ns) {
+                const wf::Sphere& s = host.spheres[p];
+                prims[3 * j] = f4(s.center, i2f(p));
+                prims[3 * j + 1] = make_float4(s.radius, 0, 0, 0);
+                prims[3 * j + 2] = make_float4(0, 0, 0, 0);
+            } else {
+                const wf::Triangle& t = host.triangles[p - ns];
+                const wf::Vec3 p0 = host.vertices[t.i0];
+                prims[3 * j] = f4(p0, i2f(p));
+                prims[3 * j + 1] = f4(host.vertices[t.i1] - p0, 0.0f);
+                prims[3 * j + 2] = f4(host.vertices[t.i2] - p0, 0.0f);
+            }
         }
-    }
-    // Spheres (wf::Sphere bytes), triangle shading records and areas, materials.
-    if (ns) std::memcpy(stage + off[kSpheres], host.spheres.data(), sizeof(wf::Sphere) * ns);
-    for (int i = 0; i < nt; ++i) {
-        const wf::Triangle& t = host.triangles[i];
-        const wf::Vec3 e1 = host.vertices[t.i1] - host.vertices[t.i0];
-        const wf::Vec3 e2 = host.vertices[t.i2] - host.vertices[t.i0];
-        tri_shade[i] = f4(wf::normalize(wf::cross(e1, e2)), i2f(t.material));
-        tri_area[i] = 0.5f * wf::length(wf::cross(e1, e2));
-    }
-    std::memcpy(stage + off[kMaterials], host.materials.data(), sizeof(wf::Material) * nm);
-    // Lights: {a, prim} {b, area} {c, material} {n, radius}.
-    for (int i = 0; i < nl; ++i) {
-        const int p = host.lights[i].prim;
-        if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "light primitive out of range");
-        if (p < ns) {
-            const wf::Sphere& s = host.spheres[p];
-            const float area = 4.0f * wf::kPi * s.radius * s.radius;
-            lights[4 * i] = f4(s.center, i2f(p));
-            lights[4 * i + 1] = make_float4(0, 0, 0, area);
-            lights[4 * i + 2] = make_float4(0, 0, 0, i2f(s.material));
-            lights[4 * i + 3] = make_float4(0, 0, 0, s.radius);
-        } else {
-            const wf::Triangle& t = host.triangles[p - ns];
-            const wf::Vec3 a = host.vertices[t.i0], b = host.vertices[t.i1], c = host.vertices[t.i2];
-            const wf::Vec3 e1 = b - a, e2 = c - a;
-            lights[4 * i] = f4(a, i2f(p));
-            lights[4 * i + 1] = f4(b, 0.5f * wf::length(wf::cross(e1, e2)));
-            lights[4 * i + 2] = f4(c, i2f(t.material));
-            lights[4 * i + 3] = f4(wf::normalize(wf::cross(b - a, c - a)), 0.0f);
+    };
+    auto pack_triangles = [&] {
+        // Triangle shading records and areas.
+        for (int i = 0; i < nt; ++i) {
+            const wf::Triangle& t = host.triangles[i];
+            const wf::Vec3 e1 = host.vertices[t.i1] - host.vertices[t.i0];
+            const wf::Vec3 e2 = host.vertices[t.i2] - host.vertices[t.i0];
+            tri_shade[i] = f4(wf::normalize(wf::cross(e1, e2)), i2f(t.material));
+            tri_area[i] = 0.5f * wf::length(wf::cross(e1, e2));
         }
-    }
+    };
+    auto pack_rest = [&] {
+        // Spheres (wf::Sphere bytes), materials and lights.
+        if (ns) std::memcpy(stage + off[kSpheres], host.spheres.data(), sizeof(wf::Sphere) * ns);
+        std::memcpy(stage + off[kMaterials], host.materials.data(), sizeof(wf::Material) * nm);
+        // Lights: {a, prim} {b, area} {c, material} {n, radius}.
+        for (int i = 0; i < nl; ++i) {
+            const int p = host.lights[i].prim;
+            if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "light primitive out of range");
+            if (p < ns) {
+                const wf::Sphere& s = host.spheres[p];
+                const float area = 4.0f * wf::kPi * s.radius * s.radius;
+                lights[4 * i] = f4(s.center, i2f(p));
+                lights[4 * i + 1] = make_float4(0, 0, 0, area);
+                lights[4 * i + 2] = make_float4(0, 0, 0, i2f(s.material));
+                lights[4 * i + 3] = make_float4(0, 0, 0, s.radius);
+            } else {
+                const wf::Triangle& t = host.triangles[p - ns];
+                const wf::Vec3 a = host.vertices[t.i0], b = host.vertices[t.i1], c = host.vertices[t.i2];
+                const wf::Vec3 e1 = b - a, e2 = c - a;
+                lights[4 * i] = f4(a, i2f(p));
+                lights[4 * i + 1] = f4(b, 0.5f * wf::length(wf::cross(e1, e2)));
+                lights[4 * i + 2] = f4(c, i2f(t.material));
+                lights[4 * i + 3] = f4(wf::normalize(wf::cross(b - a, c - a)), 0.0f);
+            }
+        }
+    };
+    run_sections({pack_nodes, pack_prims, pack_triangles, pack_rest}, (size_t)nn + np + nt > (1u << 16));
 
     auto rs = std::make_shared<ResidentScene>();
     cuda_check(cudaGetDevice(&rs->device), "cudaGetDevice");
     const size_t n_chunks = (total / 8 + kHashChunkWords - 1) / kHashChunkWords;
-    cuda_check(cudaMalloc(&rs->arena, total + n_chunks * 8), "cudaMalloc scene");
+    // From the stream-ordered pool (on the legacy stream, which orders the copy, the hash and the
+    // read-back below): a scene created per frame reuses the memory of the one before it.
+    cuda_check(cudaMallocAsync(&rs->arena, total + n_chunks * 8, 0), "allocate scene");
     rs->bytes = total;
     char* base = static_cast<char*>(rs->arena);
-    cuda_check(cudaMemcpy(base, stage, total, cudaMemcpyHostToDevice), "cudaMemcpy scene");
+    cuda_check(cudaMemcpyAsync(base, stage, total, cudaMemcpyHostToDevice, 0), "cudaMemcpy scene");
     // Content key: chunk hashes of the arena (in the tail of the same allocation), folded here.
     unsigned long long* chunk_hash = reinterpret_cast<unsigned long long*>(base + total);
-    hash_chunks<<<(unsigned)((n_chunks + 255) / 256), 256>>>(reinterpret_cast<const unsigned long long*>(base),
-                                                              total / 8, chunk_hash);
+    (void)cudaGetLastError();  // the check below is for this launch only
+    hash_chunks<<<(unsigned)((n_chunks + 255) / 256), 256, 0, 0>>>(
+        reinterpret_cast<const unsigned long long*>(base), total / 8, chunk_hash);
     cuda_check(cudaGetLastError(), "hash_chunks launch");
     std::vector<unsigned long long> hashes(n_chunks);
     cuda_check(cudaMemcpy(hashes.data(), chunk_hash, n_chunks * 8, cudaMemcpyDeviceToHost), "cudaMemcpy hashes");

@@ -68,17 +68,20 @@ Renderer::Renderer(std::shared_ptr<ResidentScene> scene, wf::GpuMode mode)
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaEventCreate(&ev0_), "cudaEventCreate");
     cuda_check(cudaEventCreate(&ev1_), "cudaEventCreate");
-    cuda_check(cudaMalloc(&counters_, sizeof(DevCounters)), "cudaMalloc counters");
-    cuda_check(cudaMalloc(&work_, 256), "cudaMalloc work counter");
     keep_pool_memory();
+    // Counters and the work counter share one block from the stream-ordered pool.
+    const size_t cbytes = (sizeof(DevCounters) + 255) & ~(size_t)255;
+    char* block = nullptr;
+    cuda_check(cudaMallocAsync(reinterpret_cast<void**>(&block), cbytes + 256, stream_), "allocate counters");
+    counters_ = reinterpret_cast<DevCounters*>(block);
+    work_ = reinterpret_cast<unsigned int*>(block + cbytes);
     alloc_film();
 }
 
 Renderer::~Renderer() {
     free_film();
     wf_.reset();
-    if (counters_) cudaFree(counters_);
-    if (work_) cudaFree(work_);
+    if (counters_) cudaFreeAsync(counters_, stream_);  // work_ is part of the same block
     if (lbuf_) cudaFreeAsync(lbuf_, stream_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
