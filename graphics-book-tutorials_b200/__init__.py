@@ -93,7 +93,8 @@ class _CRenderStats(ctypes.Structure):
                 ("queue_high_water", ctypes.c_int64 * 5), ("queue_overflows", ctypes.c_int64),
                 ("invalid_hits", ctypes.c_int64), ("peak_vram_bytes", ctypes.c_uint64),
                 ("stage_ms", ctypes.c_double * 8), ("node_visits", ctypes.c_uint64),
-                ("prim_tests", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64)]
+                ("prim_tests", ctypes.c_uint64), ("kernel_launches", ctypes.c_uint64),
+                ("kernel_ms", ctypes.c_double)]
 
 
 STAGE_NAMES = ("extend", "classify", "shade_lambert", "shade_metal", "shade_dielectric", "shadow",
@@ -141,13 +142,14 @@ class RenderStats:
     node_visits: int = 0  # megakernel with count_rays: BVH nodes visited
     prim_tests: int = 0   # megakernel with count_rays: primitive tests
     kernel_launches: int = 0  # kernels of the library launched by the call
+    kernel_ms: float = 0.0    # device time of the main kernel launches alone (CUDA events)
 
     @classmethod
     def _from_c(cls, c: _CRenderStats) -> "RenderStats":
         return cls(c.render_ms, c.total_ms, int(c.extension_rays), int(c.shadow_rays),
                    [int(v) for v in c.queue_high_water], int(c.queue_overflows), int(c.invalid_hits),
                    int(c.peak_vram_bytes), {n: float(c.stage_ms[i]) for i, n in enumerate(STAGE_NAMES)},
-                   int(c.node_visits), int(c.prim_tests), int(c.kernel_launches))
+                   int(c.node_visits), int(c.prim_tests), int(c.kernel_launches), float(c.kernel_ms))
 
 
 @dataclass

@@ -115,6 +115,7 @@ void to_c_stats(const wf::RenderStats& s, wfb_render_stats* out) {
     out->node_visits = 0;
     out->prim_tests = 0;
     out->kernel_launches = 0;
+    out->kernel_ms = 0.0;
 }
 
 void need(bool ok, const char* msg) {
@@ -352,6 +353,7 @@ int wfb_renderer_run_passes(wfb_renderer_t r, int first_sample, int count, const
             stats->node_visits = r->r->last_node_visits();
             stats->prim_tests = r->r->last_prim_tests();
             stats->kernel_launches = (uint64_t)r->r->last_kernel_launches();
+            stats->kernel_ms = r->r->last_kernel_ms();
         }
     });
 }
@@ -391,6 +393,7 @@ int wfb_renderer_render(wfb_renderer_t r, const wfb_render_params* p, wfb_render
             stats->node_visits = r->r->last_node_visits();
             stats->prim_tests = r->r->last_prim_tests();
             stats->kernel_launches = (uint64_t)r->r->last_kernel_launches();
+            stats->kernel_ms = r->r->last_kernel_ms();
         }
     });
 }

@@ -76,12 +76,30 @@ inline uint64_t split_buffer_bytes(long long pixels, long long samples) {
 int megakernel_resident_threads(const MegakernelConfig& cfg);
 // Work units per pixel (1 = direct film accumulation; > 1 needs a per-sample buffer).
 int megakernel_split_chunks(int pixels, int sample_count, const MegakernelConfig& cfg);
+
+// CUDA-event timing of a render's main kernel launches (the persistent megakernel or wavefront
+// kernel alone: no memsets, pool init, counter folds or film commits), summed over the launches of
+// one render. Events are created on first use and reused.
+class KernelTimer {
+public:
+    KernelTimer() = default;
+    KernelTimer(const KernelTimer&) = delete;
+    KernelTimer& operator=(const KernelTimer&) = delete;
+    ~KernelTimer();
+    void reset() { used_ = 0; }
+    void begin(cudaStream_t stream);  // records before a main launch
+    void end(cudaStream_t stream);    // records after it
+    double total_ms() const;          // once the stream has passed the last end()
+private:
+    std::vector<cudaEvent_t> ev_;
+    int used_ = 0;
+};
 // Adds samples [first, first + count) of every pixel to `film`. With chunks > 1, `lbuf` must hold
 // 3 * pixels * count floats (per-sample radiance, committed in sample order after the kernel).
 // Returns the number of kernels launched.
 int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters,
                        unsigned int* work_counter, float* lbuf, const PassParams& p,
-                      const MegakernelConfig& cfg, int chunks, cudaStream_t stream);
+                      const MegakernelConfig& cfg, int chunks, cudaStream_t stream, KernelTimer* timer = nullptr);
 
 // Adds per-(pixel, sample) radiance slots (3 floats, pixel-major, `count` samples per pixel) to the
 // film sums in ascending sample order (megakernel.cu).
@@ -170,6 +188,7 @@ public:
     uint64_t last_prim_tests() const { return last_prim_tests_; }
     // Kernels of this library launched by the last run_passes.
     int last_kernel_launches() const { return last_launches_; }
+    double last_kernel_ms() const { return last_kernel_ms_; }  // main kernel launches of the last pass
     // Reference download convention (WVM/src/gpu/gpu_renderer.cu:306-341).
     void download(int spp_done, float* rgb, float* lum_var);
     void download_mean(int spp_done, float* rgb);
@@ -203,6 +222,8 @@ private:
     WavefrontConfig wf_cfg_{};
     uint64_t last_node_visits_ = 0, last_prim_tests_ = 0;
     int last_launches_ = 0;
+    double last_kernel_ms_ = 0.0;
+    KernelTimer ktimer_;
     struct Wavefront;
     std::unique_ptr<Wavefront> wf_;
 };

@@ -462,7 +462,7 @@ JobDesc make_job(const DevScene& s, const DevFilm& film, float* lbuf, int first_
 
 int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* counters, unsigned int* work_counter,
                       float* lbuf, const PassParams& p, const MegakernelConfig& cfg, int chunks,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, KernelTimer* timer) {
     if (p.sample_count <= 0 || film.pixels <= 0) return 0;
     if (chunks > 1 && lbuf == nullptr) throw Error(WFB_ERR_INTERNAL, "split megakernel needs a sample buffer");
     MkArgs args{};
@@ -475,7 +475,9 @@ int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* count
     args.min_active = cfg.min_active;
     args.leaf_batch = cfg.leaf_batch;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
+    if (timer) timer->begin(stream);
     launch_any<false>(args, args.job0.units, cfg, args.job0.chunks > 1, stream);
+    if (timer) timer->end(stream);
     if (args.job0.chunks > 1) {
         launch_film_commit(film, lbuf, p.sample_count, stream);
         return 2;
@@ -505,6 +507,34 @@ void launch_film_commit_jobs(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
     film_commit_jobs<<<dim3((unsigned)sms, (unsigned)std::max(1, max_jobs)), 256, 0, stream>>>(d_jobs, d_hdr);
     cuda_check(cudaGetLastError(), "film commit launch");
+}
+
+KernelTimer::~KernelTimer() {
+    for (cudaEvent_t e : ev_) cudaEventDestroy(e);
+}
+
+void KernelTimer::begin(cudaStream_t stream) {
+    while ((int)ev_.size() < used_ + 2) {
+        cudaEvent_t e = nullptr;
+        cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        ev_.push_back(e);
+    }
+    cuda_check(cudaEventRecord(ev_[used_], stream), "cudaEventRecord");
+}
+
+void KernelTimer::end(cudaStream_t stream) {
+    cuda_check(cudaEventRecord(ev_[used_ + 1], stream), "cudaEventRecord");
+    used_ += 2;
+}
+
+double KernelTimer::total_ms() const {
+    double ms = 0.0;
+    for (int i = 0; i + 1 < used_; i += 2) {
+        float t = 0.f;
+        cuda_check(cudaEventElapsedTime(&t, ev_[i], ev_[i + 1]), "cudaEventElapsedTime");
+        ms += t;
+    }
+    return ms;
 }
 
 }  // namespace wfb

@@ -152,6 +152,8 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
             }
         }
     }
+    if (mode_ == wf::GpuMode::Wavefront) wf_->engine.reserve(pixels(), p.sample_count);
+    ktimer_.reset();
     cuda_check(cudaEventRecord(ev0_, stream_), "cudaEventRecord");
     if (mode_ == wf::GpuMode::Megakernel) {
         last_launches_ = 0;
@@ -162,10 +164,12 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
             const int chunks = megakernel_split_chunks(pixels(), q.sample_count, mk_cfg_);
             if (chunks > 1 && 3 * (size_t)pixels() * (size_t)q.sample_count > lbuf_floats_)
                 throw Error(WFB_ERR_INTERNAL, "sample buffer smaller than a sub-pass");
-            last_launches_ += launch_megakernel(view_, film_, counters_, work_, lbuf_, q, mk_cfg_, chunks, stream_);
+            last_launches_ +=
+                launch_megakernel(view_, film_, counters_, work_, lbuf_, q, mk_cfg_, chunks, stream_, &ktimer_);
         }
     } else {
-        last_launches_ = wf_->engine.run(view_, film_, counters_, p, stats ? &stats->stages : nullptr, stream_);
+        last_launches_ =
+            wf_->engine.run(view_, film_, counters_, p, stats ? &stats->stages : nullptr, stream_, &ktimer_);
     }
     cuda_check(cudaEventRecord(ev1_, stream_), "cudaEventRecord");
     cuda_check(cudaEventSynchronize(ev1_), "render");
@@ -173,6 +177,7 @@ void Renderer::run_passes(const PassParams& p, wf::RenderStats* stats) {
     cuda_check(cudaMemcpy(&c, counters_, sizeof(c), cudaMemcpyDeviceToHost), "download counters");
     if (c.error != kErrNone)
         throw Error(WFB_ERR_DEVICE_WAIT, "a bounded device-side wait gave up; the render is incomplete");
+    last_kernel_ms_ = ktimer_.total_ms();
     last_node_visits_ = c.node_visits;
     last_prim_tests_ = c.prim_tests;
     if (stats) {

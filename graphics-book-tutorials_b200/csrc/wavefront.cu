@@ -625,7 +625,7 @@ namespace {
 // Control reset, pool init, the cooperative launch and the counter fold; returns kernels launched.
 template <bool MULTI>
 int launch_pool(const WfArgs& args, int grid, int capacity, DevCounters* counters, bool count_rays,
-                cudaStream_t stream) {
+                cudaStream_t stream, KernelTimer* timer = nullptr) {
     const Pool& pool = args.pool;
     cuda_check(cudaMemsetAsync(pool.ctl, 0, sizeof(Control), stream), "memset control");
     cuda_check(cudaMemsetAsync(pool.status, 0, ((size_t)capacity / kWfBlock + 2) * sizeof(unsigned long long), stream),
@@ -634,9 +634,11 @@ int launch_pool(const WfArgs& args, int grid, int capacity, DevCounters* counter
     cuda_check(cudaGetLastError(), "wavefront init launch");
     WfArgs a = args;
     void* params[] = {&a};
+    if (timer) timer->begin(stream);
     cuda_check(cudaLaunchCooperativeKernel((const void*)wavefront_persistent<MULTI>, dim3(grid), dim3(kWfBlock), params,
                                            0, stream),
                "wavefront cooperative launch");
+    if (timer) timer->end(stream);
     wavefront_fold<<<1, 1, 0, stream>>>(pool.ctl, counters, count_rays ? 1 : 0);
     cuda_check(cudaGetLastError(), "wavefront fold launch");
     return 3;
@@ -644,27 +646,36 @@ int launch_pool(const WfArgs& args, int grid, int capacity, DevCounters* counter
 
 }  // namespace
 
+// One sample per unit while the per-sample buffer fits (as in the megakernel: consecutive slots get
+// neighbouring pixels at the same sample, and a slot takes new work after every path); otherwise a
+// pixel's samples are split only as far as needed to fill the pool.
+int WavefrontEngine::chunks_for(int pixels, int sample_count) const {
+    if (split_buffer_bytes(pixels, sample_count) <= kSplitBufferBytes) return sample_count;
+    if (pixels < capacity_) return std::min(sample_count, (capacity_ + pixels - 1) / pixels);
+    return 1;
+}
+
+void WavefrontEngine::reserve(int pixels, int sample_count) {
+    State& st = *state_;
+    if (pixels <= 0 || sample_count <= 0 || chunks_for(pixels, sample_count) <= 1) return;
+    const size_t need = 3 * (size_t)pixels * (size_t)sample_count;
+    if (need <= st.lbuf_floats) return;
+    if (st.lbuf) cudaFree(st.lbuf);
+    st.lbuf = nullptr;
+    st.lbuf_floats = 0;
+    cuda_check(cudaMalloc(&st.lbuf, need * sizeof(float)), "cudaMalloc wavefront sample buffer");
+    st.lbuf_floats = need;
+}
+
 int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
-                         wf::StageTimes* stages, cudaStream_t stream) {
+                         wf::StageTimes* stages, cudaStream_t stream, KernelTimer* timer) {
     if (p.sample_count <= 0 || film.pixels <= 0) return 0;
     State& st = *state_;
-    // One sample per unit while the per-sample buffer fits (as in the megakernel: consecutive slots
-    // get neighbouring pixels at the same sample, and a slot takes new work after every path);
-    // otherwise split a pixel's samples only as far as needed to fill the pool.
-    int chunks = 1;
-    if (split_buffer_bytes(film.pixels, p.sample_count) <= kSplitBufferBytes) chunks = p.sample_count;
-    else if (film.pixels < capacity_) chunks = std::min(p.sample_count, (capacity_ + film.pixels - 1) / film.pixels);
+    const int chunks = chunks_for(film.pixels, p.sample_count);
     WfArgs a{};
     a.job0 = make_job(s, film, nullptr, p.first_sample, p.sample_count, chunks, p.seed, p.max_depth);
     if (a.job0.chunks > 1) {
-        const size_t need = 3 * (size_t)film.pixels * (size_t)p.sample_count;
-        if (need > st.lbuf_floats) {
-            if (st.lbuf) cudaFree(st.lbuf);
-            st.lbuf = nullptr;
-            st.lbuf_floats = 0;
-            cuda_check(cudaMalloc(&st.lbuf, need * sizeof(float)), "cudaMalloc wavefront sample buffer");
-            st.lbuf_floats = need;
-        }
+        reserve(film.pixels, p.sample_count);
         a.job0.lbuf = st.lbuf;
     }
     a.jobs = nullptr;
@@ -675,7 +686,7 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
     a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = p.stage_timing ? 1 : 0;
-    int launches = launch_pool<false>(a, st.grid, capacity_, counters, p.count_rays, stream);
+    int launches = launch_pool<false>(a, st.grid, capacity_, counters, p.count_rays, stream, timer);
     if (a.job0.chunks > 1) {
         launch_film_commit(film, a.job0.lbuf, p.sample_count, stream);
         ++launches;

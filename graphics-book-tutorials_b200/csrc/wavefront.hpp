@@ -17,7 +17,10 @@ public:
     // Adds samples [p.first_sample, p.first_sample + p.sample_count) of every pixel to `film`;
     // returns the number of kernels launched.
     int run(const DevScene& s, const DevFilm& film, DevCounters* counters, const PassParams& p,
-             wf::StageTimes* stages, cudaStream_t stream);
+             wf::StageTimes* stages, cudaStream_t stream, KernelTimer* timer = nullptr);
+    // Sizes the per-sample buffer that run() needs for this many pixels and samples (run() calls
+    // it too; a caller that times run() calls it first, outside the timed region).
+    void reserve(int pixels, int sample_count);
     // Batch: every job of a device job table (units numbered across jobs, as for the batch
     // megakernel) in one cooperative launch; the caller commits split-mode films afterwards
     // (launch_film_commit_jobs). Returns the number of kernels launched.
@@ -34,6 +37,7 @@ private:
     int capacity_ = 0;
     int pixels_ = 0;
     WavefrontConfig cfg_;
+    int chunks_for(int pixels, int sample_count) const;
 };
 
 }  // namespace wfb

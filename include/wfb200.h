@@ -137,6 +137,8 @@ typedef struct {
     uint64_t node_visits; /* megakernel, with count_rays: BVH nodes visited (box tests) */
     uint64_t prim_tests;  /* megakernel, with count_rays: primitive intersection tests */
     uint64_t kernel_launches; /* kernels of this library launched by the call */
+    double kernel_ms;         /* device time of the main kernel launches alone (persistent megakernel or
+                                 wavefront kernel; CUDA events on the launching stream) */
 } wfb_render_stats; /* wf::RenderStats (WVM/include/wf/renderer.hpp:23-37) plus traversal counts */
 
 /* GpuRenderer(const Scene&, GpuMode) (WVM/src/gpu/gpu_renderer.cu:100-238). */
