@@ -31,6 +31,7 @@ PROFILE_DIR = os.path.join(ROOT, "profiles")
 
 SCENE, WIDTH, HEIGHT, SPP, DEPTH, SEED = "icospheres", 1280, 720, 64, 8, 1234
 WORKLOAD = f"{SCENE}-512 {WIDTH}x{HEIGHT} {SPP}spp depth{DEPTH} seed{SEED}"
+PROBE_SPP = 8  # tuner probes: at 2 spp the tail of a short probe ranked launch shapes unlike a 64-spp render
 METRIC = "Msamples/s per scene vs plain megakernel (bit-equal image); served p50/p99 latency"
 
 
@@ -360,7 +361,7 @@ def main():
     tuning = None
     if not args.no_tune:
         # Untimed: measured probe renders of both arms pick the arm and its launch knobs.
-        tuning = wfb.autotune(scene, WIDTH, HEIGHT, probe_spp=2, max_depth=DEPTH,
+        tuning = wfb.autotune(scene, WIDTH, HEIGHT, probe_spp=PROBE_SPP, max_depth=DEPTH,
                               try_wavefront=args.arm in ("auto", "wavefront"))
     if args.arm == "auto":
         mode = tuning.mode if tuning is not None else wfb.MEGAKERNEL
@@ -414,7 +415,7 @@ def main():
         s2 = wfb.Scene.from_arrays(host_arrays)
         r2 = wfb.GpuRenderer(s2, mode)
         if tuning is not None:  # served from the tuner's cache (same scene hash and size)
-            r2.apply_tuning(wfb.autotune(s2, WIDTH, HEIGHT, probe_spp=2, max_depth=DEPTH,
+            r2.apply_tuning(wfb.autotune(s2, WIDTH, HEIGHT, probe_spp=PROBE_SPP, max_depth=DEPTH,
                                          try_wavefront=args.arm in ("auto", "wavefront")))
         out = r2.render(params)
         dt = time.perf_counter() - t0
