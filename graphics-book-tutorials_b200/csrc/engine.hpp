@@ -42,6 +42,9 @@ uint64_t mix_key(uint64_t h, const void* data, size_t bytes);
 // (null: the calling thread's own stream, for a film whose writers have finished); returns once
 // the host buffers hold the result. rgb or lum_var may be null.
 void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream);
+// The same result converted on the host: only copy engines work on the device, so it never waits
+// for SMs held by a persistent kernel of another stream (the server's download thread uses it).
+void film_download_host(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream);
 
 // Same scene view with another camera / resolution (batch jobs and orbit cameras).
 DevScene with_camera(const DevScene& s, const wf::Camera& cam, int width, int height);

@@ -223,6 +223,31 @@ void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var
     cuda_check(es, "cudaStreamSynchronize");
 }
 
+void film_download_host(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream) {
+    if (spp_done <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "spp_done must be positive");
+    const size_t p = (size_t)film.pixels;
+    std::vector<float> lum, lum2;
+    if (rgb) cuda_check(cudaMemcpyAsync(rgb, film.rgb, 3 * p * sizeof(float), cudaMemcpyDeviceToHost, stream), "download rgb");
+    if (lum_var) {
+        lum.resize(p);
+        lum2.resize(p);
+        cuda_check(cudaMemcpyAsync(lum.data(), film.lum, p * sizeof(float), cudaMemcpyDeviceToHost, stream), "download lum");
+        cuda_check(cudaMemcpyAsync(lum2.data(), film.lum2, p * sizeof(float), cudaMemcpyDeviceToHost, stream),
+                   "download lum2");
+    }
+    cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    // The reference's host loops (WVM/src/gpu/gpu_renderer.cu:319-336), as film_resolve does them.
+    const float inv = 1.0f / (float)spp_done;
+    if (rgb)
+        for (size_t i = 0; i < 3 * p; ++i) rgb[i] *= inv;
+    if (lum_var)
+        for (size_t i = 0; i < p; ++i) {
+            const double m = (double)lum[i] / (double)spp_done;
+            const double m2 = (double)lum2[i] / (double)spp_done;
+            lum_var[i] = (float)std::max(0.0, m2 - m * m);
+        }
+}
+
 void Renderer::download(int spp_done, float* rgb, float* lum_var) { film_download(film_, spp_done, rgb, lum_var, stream_); }
 
 void Renderer::download_mean(int spp_done, float* rgb) { download(spp_done, rgb, nullptr); }

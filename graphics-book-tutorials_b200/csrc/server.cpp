@@ -417,7 +417,7 @@ void Server::downloader() {
             j->rgb.resize(3 * p);
             j->lum_var.resize(p);
             cuda_check(se, "cudaStreamCreate download");
-            film_download(j->buf.film, j->spec.sample_count, j->rgb.data(), j->lum_var.data(), dl_stream);
+            film_download_host(j->buf.film, j->spec.sample_count, j->rgb.data(), j->lum_var.data(), dl_stream);
         } catch (const std::exception& e) {
             err = e.what();
         }

@@ -43,7 +43,7 @@ def test_faster_than_reference_megakernel_with_equal_image(ref, scene, w, h, spp
     sc = wfb.Scene.generate(scene, w, h, 1234, 16)
     arrays = sc.export()
     params = wfb.RenderParams(spp=spp, seed=1234, max_depth=8)
-    tune = wfb.autotune(sc, w, h, probe_spp=2, max_depth=8, try_wavefront=True)
+    tune = wfb.autotune(sc, w, h, probe_spp=8, max_depth=8, try_wavefront=True)
     mk = wfb.GpuRenderer(sc, wfb.MEGAKERNEL)
     mk.apply_tuning(tune)
     mk_ms, img = _best_ms(mk, params)
