@@ -28,3 +28,23 @@ def test_cpu_mode_is_refused_without_fallback():
 def test_unknown_scene_is_an_error():
     p = run("render", "--scene", "no-such-scene", "--mode", "megakernel", "--width", "8", "--height", "8")
     assert p.returncode == 1 and "unknown scene" in p.stderr
+
+
+def test_batch_and_serve_reject_bad_arguments_and_job_lists(tmp_path):
+    """`wf batch` / `wf serve`: argument and job-list errors exit 1 before any device work."""
+    p = run("serve")
+    assert p.returncode == 1 and "--jobs is required" in p.stderr and "Usage: batch" in p.stderr
+    p = run("batch", "--jobs", "x.json", "--mode", "cpu")
+    assert p.returncode == 1 and "--mode must be megakernel or wavefront" in p.stderr
+    p = run("serve", "--jobs", "x.json", "--lambda", "fast")
+    assert p.returncode == 1 and "--lambda expects a number" in p.stderr
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"jobs": [{"scene": "cornell36", "width": 8}]}')
+    p = run("batch", "--jobs", str(bad))
+    assert p.returncode == 1 and "job 0 misses a field" in p.stderr
+    bad.write_text('{"jobs": [{"scene": "teapot", "width": 8, "height": 8, "spp": 1, "max_depth": 8, "seed": 1,'
+                   ' "cam_position": [0, 1, 5], "cam_look_at": [0, 0, 0], "cam_up": [0, 1, 0], "cam_vfov_deg": 50}]}')
+    p = run("batch", "--jobs", str(bad))
+    assert p.returncode == 1 and "not a benchmark generator" in p.stderr
+    p = run("batch", "--jobs", str(tmp_path / "missing.json"))
+    assert p.returncode == 1 and "cannot read" in p.stderr
