@@ -466,6 +466,10 @@ def main():
         scenes = mix_scenes(wfb)
         line["batched"] = bench_batch(wfb, scenes, repeats=1)
         line["served"] = bench_serve(wfb, scenes, lam=10.0, duration=10.0, drain=20.0)
+        # near saturation, where continuous batching and one launch per job part ways
+        line["served_lambda50"] = {
+            "continuous_batching": bench_serve(wfb, scenes, lam=50.0, duration=10.0, drain=30.0),
+            "one_job_per_launch": bench_serve(wfb, scenes, lam=50.0, duration=10.0, drain=30.0, plain=True)}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wfb)
     if rank == 0:
