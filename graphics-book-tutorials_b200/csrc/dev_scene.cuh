@@ -62,6 +62,13 @@ WF_HD int f2i(float f) {
 #endif
 }
 
+// Split-mode radiance slots (3 floats per (pixel, sample) of a call), sample-major: the slots of
+// one sample of neighbouring pixels are adjacent, so a warp of neighbouring pixels writes (and the
+// ordered commit reads) one contiguous run instead of scattered 12-byte pieces.
+WF_HD size_t sample_slot(int pixel, int sample_index, int pixels) {
+    return 3 * ((size_t)sample_index * (size_t)pixels + (size_t)pixel);
+}
+
 // ---- accessors used by the estimator templates (wf/path_core.hpp) ----
 WF_HD wf::Sphere load_sphere(const DevScene& s, int i) {
     const float4 a = ro_load(&s.spheres[2 * i]);

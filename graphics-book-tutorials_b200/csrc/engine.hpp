@@ -104,7 +104,7 @@ int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* count
                        unsigned int* work_counter, float* lbuf, const PassParams& p,
                       const MegakernelConfig& cfg, int chunks, cudaStream_t stream, KernelTimer* timer = nullptr);
 
-// Adds per-(pixel, sample) radiance slots (3 floats, pixel-major, `count` samples per pixel) to the
+// Adds per-(pixel, sample) radiance slots (3 floats, sample-major: sample_slot) to the
 // film sums in ascending sample order (megakernel.cu).
 void launch_film_commit(const DevFilm& film, const float* lbuf, int count, cudaStream_t stream);
 

@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
             }
             if (path_done) {
                 if (SPLIT || J.chunks > 1) {
-                    float* slot = J.lbuf + 3 * ((size_t)pixel * J.sample_count + (sample - J.first_sample));
+                    float* slot = J.lbuf + sample_slot(pixel, sample - J.first_sample, J.film.pixels);
                     slot[0] = ps.L.x;
                     slot[1] = ps.L.y;
                     slot[2] = ps.L.z;
@@ -329,8 +329,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
 __device__ __forceinline__ void commit_pixel(const DevFilm& film, const float* __restrict__ lbuf, int p, int count) {
     float r = film.rgb[3 * p], g = film.rgb[3 * p + 1], b = film.rgb[3 * p + 2];
     float l1 = film.lum[p], l2 = film.lum2[p];
-    const float* slot = lbuf + 3 * (size_t)p * count;
-    for (int k = 0; k < count; ++k, slot += 3) {
+    for (int k = 0; k < count; ++k) {
+        const float* slot = lbuf + sample_slot(p, k, film.pixels);
         const wf::Vec3 L{slot[0], slot[1], slot[2]};
         r += L.x;
         g += L.y;

@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                         // commit the finished sample (film_add order, WVM/src/gpu/engine.cuh:25-32)
                         const float4 l = P.rad[slot];
                         if (split) {
-                            float* dst = J.lbuf + 3 * ((size_t)u.x * J.sample_count + (u.y - J.first_sample));
+                            float* dst = J.lbuf + sample_slot(u.x, u.y - J.first_sample, J.film.pixels);
                             dst[0] = l.x;
                             dst[1] = l.y;
                             dst[2] = l.z;
