@@ -6,6 +6,8 @@
 #include <cerrno>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
+#include <thread>
 #include <fstream>
 #include <stdexcept>
 #include <string>
@@ -15,7 +17,8 @@
 namespace wf {
 namespace {
 
-// The file is read whole and parsed in place: a line is [p, end), tokens are runs of characters
+// The file is read whole and parsed in place (in chunks of whole lines on several threads for large
+// files): a line is [p, end), tokens are runs of characters
 // other than ' ', '\t' and '\r', and a '#' ends the line. Numbers are converted with strtof / strtol
 // straight from the buffer (the buffer is NUL-terminated, and a token is always followed by a
 // character that neither function consumes), so large meshes parse without a string per field.
@@ -70,6 +73,83 @@ bool face_index(const Token& t, long* out) {
     return true;
 }
 
+// A run of whole lines parsed on its own: vertices and fan triangles in file order, or the first
+// error (its 1-based line number and message). `first_line` and `vertex_base` are the number of
+// lines and of `v` statements before the run, so indices and messages are those of a serial parse.
+struct Chunk {
+    const char* b = nullptr;
+    const char* e = nullptr;
+    int first_line = 0, lines = 0;
+    size_t vertex_base = 0, v_lines = 0;
+    std::vector<Vec3> vertices;
+    std::vector<Triangle> triangles;
+    int error_line = 0;
+    std::string error;
+};
+
+// Calls fn(line_begin, line_end_before_comment) for every line of [p, end), as std::getline would
+// split them (no empty line after a final '\n'); stops early when fn returns false.
+template <class F>
+void for_lines(const char* p, const char* end, F&& fn) {
+    while (p < end) {
+        const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(end - p)));
+        const char* line_end = nl ? nl : end;
+        const char* next = nl ? nl + 1 : end;
+        const char* hash = static_cast<const char*>(std::memchr(p, '#', (size_t)(line_end - p)));
+        if (!fn(p, hash ? hash : line_end)) return;
+        p = next;
+    }
+}
+
+void parse_chunk(Chunk& c) {
+    std::vector<Token> tok(64);
+    std::vector<int> idx;
+    int n = c.first_line;
+    auto fail = [&](const std::string& what) {
+        c.error_line = n;
+        c.error = what;
+        return false;
+    };
+    for_lines(c.b, c.e, [&](const char* p, const char* line_end) {
+        ++n;
+        size_t nt = tokenize(p, line_end, tok.data(), tok.size());
+        if (nt > tok.size()) {  // a face with very many corners
+            tok.resize(nt);
+            nt = tokenize(p, line_end, tok.data(), tok.size());
+        }
+        if (nt == 0) return true;
+        if (tok[0].is("v")) {
+            if (nt != 4) return fail("a vertex needs exactly 3 coordinates");
+            Vec3 v;
+            if (!whole_float(tok[1], &v.x) || !whole_float(tok[2], &v.y) || !whole_float(tok[3], &v.z))
+                return fail("malformed vertex coordinate");
+            c.vertices.push_back(v);
+        } else if (tok[0].is("f")) {
+            if (nt < 4) return fail("a face needs at least 3 indices");
+            const long seen = (long)(c.vertex_base + c.vertices.size());
+            idx.clear();
+            for (size_t k = 1; k < nt; ++k) {
+                long v = 0;
+                if (!face_index(tok[k], &v)) return fail("malformed face index '" + tok[k].str() + "'");
+                if (v < 1 || v > seen) return fail("face index " + std::to_string(v) + " outside 1.." + std::to_string(seen));
+                idx.push_back((int)v - 1);
+            }
+            for (size_t k = 1; k + 1 < idx.size(); ++k) c.triangles.push_back(Triangle{idx[0], idx[k], idx[k + 1], 0});
+        }
+        return true;
+    });
+}
+
+// Lines and `v` statements of a chunk (the offsets of the chunks after it).
+void count_chunk(Chunk& c) {
+    for_lines(c.b, c.e, [&](const char* p, const char* line_end) {
+        ++c.lines;
+        while (p < line_end && is_space(*p)) ++p;
+        if (p < line_end && *p == 'v' && (p + 1 == line_end || is_space(p[1]))) ++c.v_lines;
+        return true;
+    });
+}
+
 }  // namespace
 
 Scene load_obj(const std::string& path, int width, int height) {
@@ -90,47 +170,55 @@ Scene load_obj(const std::string& path, int width, int height) {
     s.name = path;
     s.width = width;
     s.height = height;
-    auto fail = [&](int line, const std::string& what) {
-        throw std::runtime_error(path + " line " + std::to_string(line) + ": " + what);
+    // Large files are cut at line boundaries into one chunk per core: a counting pass gives each
+    // chunk its line and vertex offsets, then the chunks parse side by side.
+    const char* const text_begin = text.c_str();
+    const char* const text_end = text_begin + text.size();
+    constexpr size_t kChunkMin = 4u << 20;
+    const size_t cores = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t n_chunks = std::max<size_t>(1, std::min(cores, text.size() / kChunkMin));
+    std::vector<Chunk> chunks(n_chunks);
+    const char* p = text_begin;
+    for (size_t k = 0; k < n_chunks; ++k) {
+        const char* e = k + 1 == n_chunks ? text_end : text_begin + text.size() * (k + 1) / n_chunks;
+        if (e < p) e = p;
+        if (e < text_end) {  // extend to the end of the line
+            const char* nl = static_cast<const char*>(std::memchr(e, '\n', (size_t)(text_end - e)));
+            e = nl ? nl + 1 : text_end;
+        }
+        chunks[k].b = p;
+        chunks[k].e = e;
+        p = e;
+    }
+    auto run_all = [&](void (*fn)(Chunk&)) {
+        if (n_chunks == 1) {
+            fn(chunks[0]);
+            return;
+        }
+        std::vector<std::thread> threads;
+        for (size_t k = 1; k < n_chunks; ++k) threads.emplace_back([&, k] { fn(chunks[k]); });
+        fn(chunks[0]);
+        for (auto& t : threads) t.join();
     };
-    std::vector<Token> tok(64);
-    std::vector<int> idx;
-    const char* p = text.c_str();
-    const char* const text_end = p + text.size();
-    int n = 0;
-    while (p < text_end) {  // lines as std::getline yields them: no empty line after a final '\n'
-        const char* nl = static_cast<const char*>(std::memchr(p, '\n', (size_t)(text_end - p)));
-        const char* line_end = nl ? nl : text_end;
-        const char* next = nl ? nl + 1 : text_end;
-        ++n;
-        const char* hash = static_cast<const char*>(std::memchr(p, '#', (size_t)(line_end - p)));
-        if (hash) line_end = hash;
-        size_t nt = tokenize(p, line_end, tok.data(), tok.size());
-        if (nt > tok.size()) {  // a face with very many corners
-            tok.resize(nt);
-            nt = tokenize(p, line_end, tok.data(), tok.size());
+    if (n_chunks > 1) {
+        run_all(count_chunk);
+        for (size_t k = 1; k < n_chunks; ++k) {
+            chunks[k].first_line = chunks[k - 1].first_line + chunks[k - 1].lines;
+            chunks[k].vertex_base = chunks[k - 1].vertex_base + chunks[k - 1].v_lines;
         }
-        p = next;
-        if (nt == 0) continue;
-        if (tok[0].is("v")) {
-            if (nt != 4) fail(n, "a vertex needs exactly 3 coordinates");
-            Vec3 v;
-            if (!whole_float(tok[1], &v.x) || !whole_float(tok[2], &v.y) || !whole_float(tok[3], &v.z))
-                fail(n, "malformed vertex coordinate");
-            s.vertices.push_back(v);
-        } else if (tok[0].is("f")) {
-            if (nt < 4) fail(n, "a face needs at least 3 indices");
-            idx.clear();
-            for (size_t k = 1; k < nt; ++k) {
-                long v = 0;
-                if (!face_index(tok[k], &v)) fail(n, "malformed face index '" + tok[k].str() + "'");
-                if (v < 1 || v > (long)s.vertices.size())
-                    fail(n, "face index " + std::to_string(v) + " outside 1.." + std::to_string(s.vertices.size()));
-                idx.push_back((int)v - 1);
-            }
-            for (size_t k = 1; k + 1 < idx.size(); ++k)
-                s.triangles.push_back(Triangle{idx[0], idx[k], idx[k + 1], 0});
-        }
+    }
+    run_all(parse_chunk);
+    size_t nv = 0, ntri = 0;
+    for (const Chunk& c : chunks) {
+        if (!c.error.empty()) throw std::runtime_error(path + " line " + std::to_string(c.error_line) + ": " + c.error);
+        nv += c.vertices.size();
+        ntri += c.triangles.size();
+    }
+    s.vertices.reserve(nv);
+    s.triangles.reserve(ntri);
+    for (const Chunk& c : chunks) {
+        s.vertices.insert(s.vertices.end(), c.vertices.begin(), c.vertices.end());
+        s.triangles.insert(s.triangles.end(), c.triangles.begin(), c.triangles.end());
     }
     if (s.triangles.empty()) throw std::runtime_error(path + ": no faces");
 

@@ -79,6 +79,39 @@ int main(int argc, char** argv) {
            "face arity");
     expect(contains(error_of(write(dir, "e7.obj", "")), "no faces"), "empty file");
     expect(contains(error_of(dir + "/missing.obj"), "cannot open"), "missing file");
+    // Large files (parsed in chunks of lines on several threads): same arrays, and the first error in
+    // file order with its line number and the vertex count seen before it.
+    {
+        const int nv = 400000;  // about 9 MB of text: several chunks
+        std::string text = "# big\n";
+        for (int k = 0; k < nv; ++k) {
+            text += "v " + std::to_string(k % 1000) + ".5 " + std::to_string(k / 1000) + " -" + std::to_string(k % 7) + "\n";
+            if (k >= 2 && k % 3 == 2) text += "f " + std::to_string(k - 1) + "/1 " + std::to_string(k) + " " + std::to_string(k + 1) + "\r\n";
+        }
+        const wf::Scene s = wf::load_obj(write(dir, "big_ok.obj", text), 16, 9);
+        bool same = s.vertices.size() == (size_t)nv && s.triangles.size() == (size_t)((nv - 2 + 2) / 3);
+        for (int k = 0; same && k < nv; k += 997)
+            same = s.vertices[k].x == (float)(k % 1000) + 0.5f && s.vertices[k].y == (float)(k / 1000) &&
+                   s.vertices[k].z == -(float)(k % 7);
+        for (size_t t = 0; same && t < s.triangles.size(); t += 991) {
+            const int k = 2 + 3 * (int)t;
+            same = s.triangles[t].i0 == k - 2 && s.triangles[t].i1 == k - 1 && s.triangles[t].i2 == k;
+        }
+        expect(same, "large file: vertices and triangles in file order");
+        // a face late in the file that names a vertex defined after it; and an earlier malformed vertex
+        const std::string late = text + "f 1 2 " + std::to_string(nv + 1) + "\nv 0 0 0\n";
+        const int late_line = 1 + nv + (nv - 1) / 3 + 1;
+        expect(contains(error_of(write(dir, "big_late.obj", late)),
+                        "line " + std::to_string(late_line) + ": face index " + std::to_string(nv + 1) + " outside 1.." +
+                            std::to_string(nv)),
+               "large file: face index past the vertices seen so far");
+        std::string two = text;
+        two.insert(two.size() / 4, "\nv 1 2\n");  // an error in an early chunk ...
+        two += "f 0 1 2\n";                       // ... wins over one in the last chunk
+        const std::string e2 = error_of(write(dir, "big_two.obj", two));
+        expect(contains(e2, "a vertex needs exactly 3 coordinates") && !contains(e2, "malformed face index"),
+               "large file: the first error in file order is reported");
+    }
     std::printf("obj loader checks: %d failed\n", g_failed);
     return g_failed == 0 ? 0 : 1;
 }
