@@ -196,7 +196,7 @@ def mix_scenes(wfb):
 
 
 def bench_batch(wfb, scenes, n_jobs=64, repeats=2):
-    """Config 4: the 64-job mix in one persistent launch (graph replay) vs the same jobs rendered
+    """The 64-job mix in one persistent launch (graph replay) vs the same jobs rendered
     one job per launch through GpuRenderer, on the same GPU. Device time for both."""
     mix = wfb.job_mix(n_jobs, SEED)
     jobs = [(scenes[m["scene"]], wfb.mix_job_desc(m, scenes[m["scene"]])) for m in mix]
@@ -234,7 +234,7 @@ def bench_batch(wfb, scenes, n_jobs=64, repeats=2):
 
 
 def sweep_batch(wfb, scenes, n_jobs=64):
-    """Config 4 sweep: the 64-job mix in one launch per configuration -- megakernel block
+    """Launch-shape sweep: the 64-job mix in one launch per configuration -- megakernel block
     {64, 128, 256} and wavefront paths in flight {256K, 512K, 1M, 2M, 4M, 8M}. Yields one dict each."""
     mix = wfb.job_mix(n_jobs, SEED)
     jobs = [(scenes[m["scene"]], wfb.mix_job_desc(m, scenes[m["scene"]])) for m in mix]
@@ -255,7 +255,7 @@ def sweep_batch(wfb, scenes, n_jobs=64):
 
 
 def bench_serve(wfb, scenes, lam, duration, drain=30.0, plain=False, seed=SEED, target_ms=20.0):
-    """Config 5: open-loop Poisson arrivals at `lam` jobs/s for `duration` s from the config-4 mix;
+    """Served jobs: open-loop Poisson arrivals at `lam` jobs/s for `duration` s from the 64-job mix;
     latency = submit -> film on the host. Jobs still running `drain` s after the last arrival are
     reported as incomplete (and their latency is not in the percentiles)."""
     import threading
@@ -315,7 +315,7 @@ def main():
     ap.add_argument("--size", default=None, help="WxH override (profiling cases only; not a bench line)")
     ap.add_argument("--spp", type=int, default=None, help="spp override (profiling cases only)")
     ap.add_argument("--mode", default="render", choices=["render", "batch", "serve"],
-                    help="render: config 2 headline line; batch: config 4; serve: config 5 lambda sweep")
+                    help="render: the icospheres 1280x720 64-spp line; batch: the 64-job mix; serve: a sweep of arrival rates")
     ap.add_argument("--lambdas", default="5,10,20,50,100,200")
     ap.add_argument("--duration", type=float, default=60.0)
     ap.add_argument("--no-batch-serve", action="store_true", help="skip the batched/served summary in render mode")
@@ -345,7 +345,7 @@ def main():
             for row in sweep_batch(wfb, scenes):
                 print(json.dumps(row), flush=True)
                 best = row if best is None or row["msamples_s"] > best["msamples_s"] else best
-            out = {"mode": "batch", "workload": "config-4 job mix (64 jobs, seed 1234)", **bench_batch(wfb, scenes),
+            out = {"mode": "batch", "workload": "64-job mix (seed 1234)", **bench_batch(wfb, scenes),
                    "best_of_sweep": best}
             out["device"] = wfb.device_name()
             print(json.dumps(out), flush=True)

@@ -54,7 +54,7 @@ def test_batch_jobs_equal_solo_renders(wfb, scenes):
 
 @pytest.mark.parametrize("pool", [1 << 12, 1 << 20])
 def test_wavefront_batch_jobs_equal_solo_renders(wfb, scenes, pool):
-    """Config 4 on the other arm: the paths of every job share one persistent wavefront pool (each
+    """The 64-job batch on the other arm: the paths of every job share one persistent wavefront pool (each
     slot carries its job); small pools force split jobs and slot reuse across jobs."""
     jobs = small_jobs(wfb, scenes, 12, seed=7)
     b = wfb.Batch(max_jobs=16, mode=wfb.WAVEFRONT, paths_in_flight=pool)

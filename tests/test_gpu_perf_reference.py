@@ -12,7 +12,7 @@ from conftest import load_engine
 pytestmark = pytest.mark.gpu
 
 CONFIGS = [
-    # scene, width, height, spp  (depth 8, seed 1234)
+    # scene, width, height, spp (the three benchmark scenes, depth 8, seed 1234)
     ("cornell36", 320, 180, 16),
     ("icospheres", 1280, 720, 64),
     ("heightfield", 1280, 720, 64),
@@ -63,7 +63,7 @@ def test_faster_than_reference_megakernel_with_equal_image(ref, scene, w, h, spp
         "reference_megakernel_ms": rst["render_ms"], "reference_megakernel_msamples_s": samples / rst["render_ms"] / 1e3,
         "reference_megakernel_wall_s": ref_wall,
     }
-    if scene != "heightfield":  # the reference wavefront needs ~0.5 GB per 1M paths; kept to configs 1-2
+    if scene != "heightfield":  # the reference wavefront needs ~0.5 GB per 1M paths; kept to the two smaller scenes
         wrgb, _, wst = ref.ref_render_gpu(arrays, 1, spp, 1234, 8)
         assert np.array_equal(wrgb.view(np.uint32), rrgb.view(np.uint32))
         result["reference_wavefront_ms"] = wst["render_ms"]
@@ -73,7 +73,7 @@ def test_faster_than_reference_megakernel_with_equal_image(ref, scene, w, h, spp
 
 
 def test_mixed_job_stream_against_reference_plain_megakernel(ref):
-    """The 64-job mix (scenes of configs 1-3, uneven resolution / spp / depth / camera): the batched
+    """The 64-job mix (the three benchmark scenes, uneven resolution / spp / depth / camera): the batched
     engine (one persistent launch, graph replay), the engine one job per launch, and the reference's
     plain megakernel one job per launch (one launch per sample) -- device time for all three, and
     every job's image bit-equal to the reference's render of the same job."""
