@@ -9,9 +9,10 @@ built by the engine's generator; no external data.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--arm megakernel|wavefront]
   python bench.py --impl reference ...   # the reference's own CPU arm on the host cores
 
-N > 1 runs N independent replicas (one process per GPU under torchrun): the path has no
-cross-GPU exchange, value = all samples rendered / max-over-ranks device time.
-Rank 0 prints one JSON line.
+N > 1 runs N independent replicas, one process per GPU: the path has no cross-GPU exchange,
+value = all samples rendered / max-over-ranks device time. Started without a launcher,
+`--gpus N` starts the N ranks itself (torch.distributed.run on 127.0.0.1); under a launcher,
+WORLD_SIZE must equal N. Rank 0 prints one JSON line.
 """
 import argparse
 import importlib.util
@@ -300,6 +301,20 @@ def bench_serve(wfb, scenes, lam, duration, drain=30.0, plain=False, seed=SEED, 
             "mode": "one-job-per-launch" if plain else "continuous-batching"}
 
 
+def free_port() -> int:
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def launch_ranks(n: int, argv) -> int:
+    """Runs this script as n ranks (one per GPU) under torch.distributed.run; returns its exit code."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={free_port()}", os.path.abspath(__file__)] + list(argv)
+    return subprocess.run(cmd).returncode
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -320,6 +335,15 @@ def main():
     ap.add_argument("--duration", type=float, default=60.0)
     ap.add_argument("--no-batch-serve", action="store_true", help="skip the batched/served summary in render mode")
     args = ap.parse_args()
+    if args.gpus < 1:
+        ap.error("--gpus must be at least 1")
+    if "WORLD_SIZE" in os.environ:
+        if int(os.environ["WORLD_SIZE"]) != args.gpus:
+            print(f"bench.py: --gpus {args.gpus} but the launcher started WORLD_SIZE={os.environ['WORLD_SIZE']} ranks",
+                  file=sys.stderr)
+            sys.exit(2)
+    elif args.gpus > 1:
+        sys.exit(launch_ranks(args.gpus, sys.argv[1:]))
     args.warmup = max(args.warmup, 3)
     global WIDTH, HEIGHT, SPP, WORKLOAD
     if args.size:

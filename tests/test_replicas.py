@@ -79,3 +79,29 @@ def test_reference_arm_runs_on_rank_zero_only():
                        capture_output=True, text=True, timeout=120, env=env)
     assert p.returncode == 0, p.stderr
     assert p.stdout.strip() == ""
+
+
+def test_bench_gpus_flag_starts_its_own_ranks():
+    """`bench.py --gpus 2` without a launcher starts two ranks itself; rank 0 alone prints the line,
+    which reports both ranks (the reference arm: rank 0 times the CPU arm, the other exits)."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2",
+                          "--steps", "1", "--warmup", "3", "--ref-spp", "1"],
+                         capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1 and lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"
+
+
+def test_bench_gpus_flag_must_match_the_launcher():
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, WORLD_SIZE="3", RANK="0")
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2"],
+                         capture_output=True, text=True, timeout=120, env=env)
+    assert out.returncode != 0 and "WORLD_SIZE=3" in out.stderr
