@@ -255,7 +255,7 @@ def sweep_batch(wfb, scenes, n_jobs=64):
                "msamples_s": round(samples / ms / 1e3, 2), "samples": samples}
 
 
-def bench_serve(wfb, scenes, lam, duration, drain=30.0, plain=False, seed=SEED, target_ms=20.0):
+def bench_serve(wfb, scenes, lam, duration, drain=30.0, plain=False, seed=SEED, target_ms=20.0, schedule="express"):
     """Served jobs: open-loop Poisson arrivals at `lam` jobs/s for `duration` s from the 64-job mix;
     latency = submit -> film on the host. Jobs still running `drain` s after the last arrival are
     reported as incomplete (and their latency is not in the percentiles)."""
@@ -263,13 +263,13 @@ def bench_serve(wfb, scenes, lam, duration, drain=30.0, plain=False, seed=SEED, 
     mix = wfb.job_mix(64, SEED)
     descs = [(scenes[m["scene"]], wfb.mix_job_desc(m, scenes[m["scene"]])) for m in mix]
     rng = np.random.default_rng(seed + int(lam * 1000))
-    srv = wfb.Server(one_job_per_launch=plain, launch_target_ms=target_ms)
+    srv = wfb.Server(one_job_per_launch=plain, launch_target_ms=target_ms, schedule=schedule)
     # warm-up: one small job (graph capture, module load)
     w = srv.submit(*descs[min(range(64), key=lambda i: descs[i][1].width * descs[i][1].height * descs[i][1].spp)])
     srv.wait(w, 60000)
     srv.result(w)
     srv.reset_stats()
-    tickets = []
+    tickets, sizes = [], []
     done_flag = threading.Event()
     t0 = time.perf_counter()
     t_next = t0
@@ -282,13 +282,16 @@ def bench_serve(wfb, scenes, lam, duration, drain=30.0, plain=False, seed=SEED, 
             time.sleep(delay)
         s, j = descs[int(rng.integers(64))]
         tickets.append(srv.submit(s, j))
+        sizes.append(j.width * j.height * j.spp)
     submitted = len(tickets)
     deadline = time.perf_counter() + drain
     completed = 0
-    for t in tickets:
+    per_job = []  # (samples, latency ms) of every finished job
+    for t, size in zip(tickets, sizes):
         left = int(max(0.0, deadline - time.perf_counter()) * 1000)
         if srv.wait(t, left):
-            srv.result(t)
+            _, lat = srv.result(t)
+            per_job.append((size, lat))
             completed += 1
     done_flag.set()
     st = srv.stats()
@@ -298,7 +301,20 @@ def bench_serve(wfb, scenes, lam, duration, drain=30.0, plain=False, seed=SEED, 
             "p99_ms": round(st["p99_ms"], 2), "mean_ms": round(st["mean_ms"], 2),
             "msamples_s": round(st["samples_done"] / max(st["wall_s"], 1e-9) / 1e6, 2),
             "busy_frac": round(st["busy_ms"] / 1e3 / max(st["wall_s"], 1e-9), 3), "launches": st["launches"],
-            "mode": "one-job-per-launch" if plain else "continuous-batching"}
+            "mode": "one-job-per-launch" if plain else "continuous-batching",
+            "schedule": None if plain else schedule, "by_size": latency_by_size(per_job)}
+
+
+def latency_by_size(per_job):
+    """p50 / p99 latency per job-size class (samples = width * height * spp)."""
+    classes = (("small<1M", 0, 1e6), ("mid<20M", 1e6, 2e7), ("large", 2e7, float("inf")))
+    out = {}
+    for name, lo, hi in classes:
+        lat = sorted(l for n, l in per_job if lo <= n < hi)
+        if lat:
+            out[name] = {"n": len(lat), "p50_ms": round(float(np.percentile(lat, 50)), 1),
+                         "p99_ms": round(float(np.percentile(lat, 99)), 1)}
+    return out
 
 
 def free_port() -> int:
@@ -333,6 +349,7 @@ def main():
                     help="render: the icospheres 1280x720 64-spp line; batch: the 64-job mix; serve: a sweep of arrival rates")
     ap.add_argument("--lambdas", default="5,10,20,50,100,200")
     ap.add_argument("--duration", type=float, default=60.0)
+    ap.add_argument("--schedules", default="express", help="serve mode: continuous-batching schedules to run")
     ap.add_argument("--no-batch-serve", action="store_true", help="skip the batched/served summary in render mode")
     args = ap.parse_args()
     if args.gpus < 1:
@@ -375,8 +392,8 @@ def main():
             print(json.dumps(out), flush=True)
         else:
             for lam in [float(x) for x in args.lambdas.split(",")]:
-                for plain in (False, True):
-                    r = bench_serve(wfb, scenes, lam, args.duration, plain=plain)
+                for plain, schedule in [(False, s) for s in args.schedules.split(",")] + [(True, "express")]:
+                    r = bench_serve(wfb, scenes, lam, args.duration, plain=plain, schedule=schedule)
                     print(json.dumps({"mode": "serve", **r}), flush=True)
         group.close()
         return
@@ -477,7 +494,12 @@ def main():
             "kernel_ms": round(kernel_ms, 3),
             "issue_active_frac": prof.get("issue_active_frac"),
             "lanes_per_instr": prof.get("lanes_per_instr"),
-            "note": "traversal is issue-bound on an L2-resident BVH; see issue_active_frac x lanes_per_instr/32",
+            # the traversal bound (issue slots used x useful lanes per issued instruction), from the
+            # committed ncu summary of this kernel
+            "issue_lane_frac": (round(prof["issue_active_frac"] * prof["lanes_per_instr"] / 32.0, 4)
+                                if "issue_active_frac" in prof and "lanes_per_instr" in prof else None),
+            "note": "traversal is issue-bound on an L2-resident BVH: issue_lane_frac = issue_active_frac x "
+                    "lanes_per_instr/32 is the fraction of the SMs' thread-instruction slots doing useful work",
         },
         "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -489,7 +511,9 @@ def main():
     if rank == 0 and not args.no_batch_serve:
         scenes = mix_scenes(wfb)
         line["batched"] = bench_batch(wfb, scenes, repeats=1)
-        line["served"] = bench_serve(wfb, scenes, lam=10.0, duration=10.0, drain=20.0)
+        line["served"] = {
+            "continuous_batching": bench_serve(wfb, scenes, lam=10.0, duration=10.0, drain=20.0),
+            "one_job_per_launch": bench_serve(wfb, scenes, lam=10.0, duration=10.0, drain=20.0, plain=True)}
         # near saturation, where continuous batching and one launch per job part ways
         line["served_lambda50"] = {
             "continuous_batching": bench_serve(wfb, scenes, lam=50.0, duration=10.0, drain=30.0),

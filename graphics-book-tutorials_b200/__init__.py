@@ -202,6 +202,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_renderer_render": (i32, [vp, ctypes.POINTER(_CRenderParams), ctypes.POINTER(_CRenderStats), vp, vp]),
         "wfb_renderer_device_bytes": (u64, [vp]),
         "wfb_renderer_configure": (i32, [vp, i32, i32, i32, i32, i32, i32, i32]),
+        "wfb_renderer_set_l2_residency": (i32, [vp, i32]),
+        "wfb_device_facts_get": (i32, [vp]),
+        "wfb_renderer_l2_window_bytes": (u64, [vp]),
         "wfb_renderer_width": (i32, [vp]),
         "wfb_renderer_height": (i32, [vp]),
         "wfb_renderer_destroy": (i32, [vp]),
@@ -211,6 +214,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_compact_u32": (i32, [vp, vp, vp, vp, vp, i32, vp, vp]),
         "wfb_test_queue_push": (i32, [vp, i32, vp, u32, vp, vp, vp]),
         "wfb_scan_workspace_check": (i32, [vp, vp]),
+        "wfb_test_bounded_wait": (i32, [ctypes.c_uint64, i32]),
         "wfb_autotune": (i32, [vp, i32, i32, i32, i32, i32, ctypes.POINTER(_CTuneResult)]),
         "wfb_renderer_apply_tuning": (i32, [vp, ctypes.POINTER(_CTuneResult)]),
     }
@@ -225,6 +229,24 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 def _check(status: int) -> None:
     if status != OK:
         raise WfbError(status, (load_library().wfb_last_error() or b"").decode())
+
+
+class _CDeviceFacts(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 256), ("driver_version", ctypes.c_int), ("runtime_version", ctypes.c_int),
+                ("cc_major", ctypes.c_int), ("cc_minor", ctypes.c_int), ("sm_count", ctypes.c_int),
+                ("total_memory_bytes", ctypes.c_uint64), ("free_memory_bytes", ctypes.c_uint64),
+                ("l2_bytes", ctypes.c_uint64), ("persisting_l2_max_bytes", ctypes.c_uint64),
+                ("access_window_max_bytes", ctypes.c_uint64), ("wavefront_l2_resident_paths", ctypes.c_int),
+                ("wavefront_slot_bytes", ctypes.c_int)]
+
+
+def device_facts() -> dict:
+    """wf::query_cuda_device (WVM/src/gpu/gpu_renderer.cu:13-56) plus the L2 figures the wavefront uses."""
+    f = _CDeviceFacts()
+    _check(load_library().wfb_device_facts_get(ctypes.byref(f)))
+    out = {k: getattr(f, k) for k, _ in _CDeviceFacts._fields_}
+    out["name"] = f.name.decode()
+    return out
 
 
 def device_name() -> str:
@@ -401,6 +423,13 @@ class GpuRenderer:
         _check(load_library().wfb_renderer_configure(self._h, block, blocks_per_sm, min_active, split_chunks,
                                                       paths_in_flight, occupancy, leaf_batch))
 
+    def set_l2_residency(self, mode: int) -> None:
+        """Wavefront pool under a persisting L2 window: -1 when it fits the set-aside, 0 never, 1 always."""
+        _check(load_library().wfb_renderer_set_l2_residency(self._h, int(mode)))
+
+    def l2_window_bytes(self) -> int:
+        return int(load_library().wfb_renderer_l2_window_bytes(self._h))
+
     def apply_tuning(self, tuning: "TuneResult") -> None:
         """Applies the knobs of an autotune result that belong to this renderer's arm."""
         _check(load_library().wfb_renderer_apply_tuning(self._h, ctypes.byref(tuning._c)))
@@ -518,6 +547,12 @@ def test_queue_push(d_flags: int, n: int, d_items: int, capacity: int, d_counter
                                               d_overflow, stream or None)
 
 
+def set_bounded_wait_test(limit_ns: int, unsatisfiable: bool = False) -> None:
+    """Test hook (wfb_test_bounded_wait): limit of every bounded device-side wait (0: the 2 s default)
+    and, with ``unsatisfiable``, a wait that never completes in the next wavefront launch or scan."""
+    _check(load_library().wfb_test_bounded_wait(int(limit_ns), 1 if unsatisfiable else 0))
+
+
 # ---------------------------------------------------------------------------------------------
 # Batched rendering and the render server (no reference counterpart).
 
@@ -540,9 +575,13 @@ def _launch_config(mode=0, use_graph=True, block=0, occupancy=-1, min_active=0, 
                           int(leaf_batch), int(paths_in_flight), int(split_chunks))
 
 
+SCHEDULES = {"express": 0, "shared": 1}  # WFB_SCHEDULE_EXPRESS, WFB_SCHEDULE_SHARED
+
+
 class _CServerConfig(ctypes.Structure):
     _fields_ = [("budget_bytes", ctypes.c_uint64), ("max_jobs", ctypes.c_int), ("launch_target_ms", ctypes.c_double),
-                ("fixed_slice", ctypes.c_int), ("one_job_per_launch", ctypes.c_int), ("launch", _CLaunchConfig)]
+                ("fixed_slice", ctypes.c_int), ("one_job_per_launch", ctypes.c_int), ("launch", _CLaunchConfig),
+                ("schedule", ctypes.c_int)]
 
 
 class _CServerStats(ctypes.Structure):
@@ -672,12 +711,14 @@ class Server:
     def __init__(self, budget_bytes: int = 0, max_jobs: int = 0, launch_target_ms: float = 0.0,
                  fixed_slice: int = 0, one_job_per_launch: bool = False, use_graph: bool = True, block: int = 0,
                  min_active: int = 0, mode: int = MEGAKERNEL, occupancy: int = -1, leaf_batch: int = 0,
-                 paths_in_flight: int = 0, split_chunks: int = 0):
+                 paths_in_flight: int = 0, split_chunks: int = 0, schedule: str = "express"):
         lib = _bind_batch_server(load_library())
+        if schedule not in SCHEDULES:
+            raise ValueError(f"schedule must be one of {sorted(SCHEDULES)}")
         cfg = _CServerConfig(int(budget_bytes), int(max_jobs), float(launch_target_ms), int(fixed_slice),
                              int(bool(one_job_per_launch)),
                              _launch_config(mode, use_graph, block, occupancy, min_active, leaf_batch, paths_in_flight,
-                                            split_chunks))
+                                            split_chunks), SCHEDULES[schedule])
         h = ctypes.c_void_p()
         _check(lib.wfb_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

@@ -10,15 +10,19 @@
 //   megakernel: stage 1, (block, occupancy target) in {(128,10), (128,8), (128,6), (128,0), (64,0), (256,0)}
 //               x min_active in {8, 16, 24} at leaf_batch 8; stage 2, the stage-1 winner with
 //               leaf_batch in {4, 12, 16, 32}
-//   wavefront:  paths in flight in {1M, 2M, 4M, 8M} x min_active {16, 24}, probed with at least 8
-//               samples so that the pool can fill; its queues are sized to
-//               the pool, so they never drop a path.
+//   wavefront:  paths in flight in {the largest pool that fits the persisting L2 set-aside (its
+//               launches carry a persisting access-policy window), 1M, 2M, 4M, 8M} x min_active
+//               {16, 24}, probed with at least 8 samples so that the pool can fill. Queue capacity is
+//               not a knob: every queue is sized to the pool, so none can drop a path (the
+//               reference's capacity knob exists to test overflow, WVM/src/gpu/wavefront.cu:279-280).
 #include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <vector>
 #include "autotune.hpp"
+#include "wavefront.hpp"
 #include "../../include/wfb200.h"
 
 namespace wfb {
@@ -92,7 +96,11 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
         }
     }
     if (try_wavefront) {
-        const int pools[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
+        int dev = 0;
+        cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        const int l2_pool = (int)wavefront_l2_resident_paths(dev);
+        std::vector<int> pools = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
+        if (l2_pool >= 1 << 16) pools.insert(pools.begin(), l2_pool);
         const int actives[] = {16, 24};
         PassParams pw = p;  // enough samples for the larger pools to fill
         pw.sample_count = std::max(probe_spp, 8);

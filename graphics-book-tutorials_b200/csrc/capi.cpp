@@ -11,6 +11,7 @@
 #include "noalloc.hpp"
 #include "queues.hpp"
 #include "server.hpp"
+#include "wavefront.hpp"
 #include "scene_gen.hpp"
 #include "../../include/wfb200.h"
 
@@ -184,6 +185,11 @@ int wfb_device_facts_get(wfb_device_facts* out) {
         out->sm_count = prop.multiProcessorCount;
         out->total_memory_bytes = total_b;
         out->free_memory_bytes = free_b;
+        out->l2_bytes = (uint64_t)prop.l2CacheSize;
+        out->persisting_l2_max_bytes = (uint64_t)prop.persistingL2CacheMaxSize;
+        out->access_window_max_bytes = (uint64_t)prop.accessPolicyMaxWindowSize;
+        out->wavefront_l2_resident_paths = (int)wfb::wavefront_l2_resident_paths(dev);
+        out->wavefront_slot_bytes = (int)wfb::wavefront_slot_bytes();
     });
 }
 
@@ -412,6 +418,16 @@ int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int m
         r->r->configure(block, blocks_per_sm, min_active, split_chunks, paths_in_flight, occupancy, leaf_batch);
     });
 }
+int wfb_renderer_set_l2_residency(wfb_renderer_t r, int mode) {
+    return guarded([&] {
+        need(r != nullptr, "null renderer");
+        need(mode >= -1 && mode <= 1, "L2 residency mode must be -1, 0 or 1");
+        r->r->set_l2_residency(mode);
+    });
+}
+
+uint64_t wfb_renderer_l2_window_bytes(wfb_renderer_t r) { return r ? r->r->l2_window_bytes() : 0; }
+
 int wfb_renderer_width(wfb_renderer_t r) { return r ? r->r->width() : 0; }
 int wfb_renderer_height(wfb_renderer_t r) { return r ? r->r->height() : 0; }
 
@@ -524,6 +540,8 @@ int wfb_server_create(const wfb_server_config* c, wfb_server_t* out) {
         if (c->launch_target_ms > 0) cfg.launch_target_ms = c->launch_target_ms;
         cfg.fixed_slice = c->fixed_slice;
         cfg.one_job_per_launch = c->one_job_per_launch != 0;
+        need(c->schedule == WFB_SCHEDULE_EXPRESS || c->schedule == WFB_SCHEDULE_SHARED, "unknown schedule");
+        cfg.schedule = c->schedule == WFB_SCHEDULE_SHARED ? wfb::kScheduleShared : wfb::kScheduleExpress;
         cfg.launch = launch_config(&c->launch);
         if (c->launch.split_chunks <= 0) cfg.launch.mk.split_chunks = wfb::kServerSplitChunks;
         auto s = std::make_unique<wfb_server>();
@@ -651,6 +669,10 @@ int wfb_scan_workspace_check(wfb_scan_workspace_t ws, void* stream) {
         if (wfb::scan_workspace_failed(*ws->ws, static_cast<cudaStream_t>(stream)))
             throw wfb::Error(WFB_ERR_DEVICE_WAIT, "a scan look-back wait gave up");
     });
+}
+
+int wfb_test_bounded_wait(uint64_t limit_ns, int unsatisfiable) {
+    return guarded([&] { wfb::set_device_wait_test(limit_ns, unsatisfiable != 0); });
 }
 
 int wfb_render_passes_noalloc(wfb_scene_t s, int first_sample, int count, uint32_t seed, int max_depth,

@@ -26,11 +26,15 @@ ResidentScene::~ResidentScene() {
         int cur = -1;
         cudaGetDevice(&cur);
         if (device >= 0 && cur != device) cudaSetDevice(device);
-        // No kernel reads the scene any more: every render and batch launch waits for its kernels
-        // before returning, and renderers and batches hold the scene while they exist.
+        // Renders and batch launches wait for their kernels before returning, and renderers and
+        // batches hold the scene while they exist; work that returned without waiting (the
+        // allocation-free entry, on the caller's stream) recorded `last_use`, which the release
+        // waits for.
+        if (last_use) cudaStreamWaitEvent(0, last_use, 0);
         cudaFreeAsync(arena, 0);
         if (device >= 0 && cur != device && cur >= 0) cudaSetDevice(cur);
     }
+    if (last_use) cudaEventDestroy(last_use);
 }
 
 namespace {
@@ -273,6 +277,7 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
 
     auto rs = std::make_shared<ResidentScene>();
     cuda_check(cudaGetDevice(&rs->device), "cudaGetDevice");
+    cuda_check(cudaEventCreateWithFlags(&rs->last_use, cudaEventDisableTiming), "cudaEventCreate scene use");
     const size_t n_chunks = (total / 8 + kHashChunkWords - 1) / kHashChunkWords;
     // From the stream-ordered pool (on the legacy stream, which orders the copy, the hash and the
     // read-back below): a scene created per frame reuses the memory of the one before it.

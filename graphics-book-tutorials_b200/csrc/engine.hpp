@@ -20,6 +20,16 @@ struct Error : std::runtime_error {
 
 void cuda_check(cudaError_t e, const char* what);  // throws Error(WFB_ERR_CUDA or OOM)
 
+// Bounded device-side waits (wavefront grid barriers, scan look-backs): a wait longer than
+// device_wait_limit_ns() gives up and the call reports WFB_ERR_DEVICE_WAIT (queues.cu).
+uint64_t device_wait_limit_ns();
+// Test hook: sets the limit (0: the 2 s default) and, with unsatisfiable_next, makes the next
+// wavefront launch or scan wait for something that never happens (a CTA the launch does not have,
+// a tile no CTA claims), so that its wait runs out.
+void set_device_wait_test(uint64_t limit_ns, bool unsatisfiable_next);
+// Consumes the pending unsatisfiable-wait request, if any.
+bool take_unsatisfiable_wait();
+
 // Scene uploaded once in the packed device layout; shared (reference-counted) by every renderer
 // and batch job that draws it, so a BVH stays resident across renders.
 struct ResidentScene {
@@ -28,6 +38,9 @@ struct ResidentScene {
     uint64_t bytes = 0;
     uint64_t content_key = 0;   // hash of the packed arena, environment and default camera
     int device = -1;
+    // Recorded after work that reads the arena on a caller's stream and returns without waiting
+    // (the allocation-free entry); the arena's release waits for it.
+    cudaEvent_t last_use = nullptr;
     ~ResidentScene();
 };
 
@@ -157,6 +170,7 @@ void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
 // ---- wavefront (wavefront.cu) ----
 struct WavefrontConfig {
     int paths_in_flight = 0;  // path-pool slots; 0: 4M (capped at 64 x pixels)
+    int l2_persist = -1;      // pool under a persisting L2 window: -1 when it fits the set-aside, 0 never, 1 always
     int min_active = 20;      // traverse on while at least this many lanes of a warp traverse
     int leaf_batch = 8;       // a warp tests primitives once this many lanes hold a pending leaf
 };
@@ -206,6 +220,10 @@ public:
     // Values < 0 keep the current setting (block and min_active also keep on 0).
     void configure(int block, int blocks_per_sm, int min_active, int split_chunks, int paths_in_flight,
                    int occupancy, int leaf_batch = -1);
+    // Wavefront pool under a persisting L2 window: -1 when it fits the set-aside, 0 never, 1 always.
+    void set_l2_residency(int mode);
+    // Bytes of the wavefront pool under the window (0: none, or a megakernel renderer).
+    uint64_t l2_window_bytes() const;
 
 private:
     void alloc_film();

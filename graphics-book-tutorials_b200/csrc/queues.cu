@@ -5,6 +5,7 @@
 //   compact  one launch: flags -> tile scan -> stable scatter (no indicator array, no second pass).
 // Tiles are claimed through an atomic ticket, so a tile only ever waits on tiles claimed before
 // it by CTAs that are already running: the look-back always makes progress.
+#include <atomic>
 #include <cstring>
 #include "engine.hpp"
 #include "queues.cuh"
@@ -23,7 +24,8 @@ constexpr int kScanTile = kScanBlock * kScanItems;
 template <int MODE>
 __global__ void __launch_bounds__(kScanBlock) scan_tiles(const uint32_t* in, const uint32_t* values, uint32_t* out,
                                                          int n, uint32_t* total, unsigned long long* status,
-                                                         unsigned* ticket, unsigned epoch, unsigned* err) {
+                                                         unsigned* ticket, unsigned epoch, unsigned* err,
+                                                         unsigned long long wait_ns) {
     __shared__ uint32_t smem[33];
     __shared__ int s_tile;
     __shared__ uint32_t s_prefix;
@@ -48,7 +50,7 @@ __global__ void __launch_bounds__(kScanBlock) scan_tiles(const uint32_t* in, con
         else publish_status(status, tile, epoch, kStatusAggregate, aggregate);
     }
     if (tile > 0 && threadIdx.x < 32) {
-        const uint32_t p = tile_lookback(status, tile, epoch, err);
+        const uint32_t p = tile_lookback(status, tile, epoch, err, wait_ns);
         if (threadIdx.x == 0) {
             publish_status(status, tile, epoch, kStatusPrefix, p + aggregate);
             s_prefix = p;
@@ -79,7 +81,31 @@ __global__ void queue_push_test_kernel(const uint32_t* flags, int n, uint32_t* i
 
 int tiles_for(int n) { return (n + kScanTile - 1) / kScanTile; }
 
+std::atomic<unsigned long long> g_wait_limit_ns{kDefaultWaitLimitNs};
+std::atomic<bool> g_unsatisfiable_next{false};
+
+// Tile tickets start at 0; a test that asked for an unsatisfiable wait starts them at 1, so no CTA
+// claims tile 0 and every look-back waits for a prefix that nothing publishes.
+void start_tickets(ScanWorkspace& ws, cudaStream_t stream) {
+    if (take_unsatisfiable_wait()) {
+        static const unsigned one = 1u;
+        cuda_check(cudaMemcpyAsync(ws.ticket, &one, sizeof(unsigned), cudaMemcpyHostToDevice, stream), "set ticket");
+        cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");  // `one` is read before returning
+    } else {
+        cuda_check(cudaMemsetAsync(ws.ticket, 0, sizeof(unsigned), stream), "memset ticket");
+    }
+}
+
 }  // namespace
+
+uint64_t device_wait_limit_ns() { return g_wait_limit_ns.load(); }
+
+void set_device_wait_test(uint64_t limit_ns, bool unsatisfiable_next) {
+    g_wait_limit_ns.store(limit_ns ? limit_ns : kDefaultWaitLimitNs);
+    g_unsatisfiable_next.store(unsatisfiable_next);
+}
+
+bool take_unsatisfiable_wait() { return g_unsatisfiable_next.exchange(false); }
 
 ScanWorkspace::~ScanWorkspace() {
     if (arena) cudaFree(arena);
@@ -107,10 +133,10 @@ void scan_exclusive_u32(const uint32_t* in, uint32_t* out, int n, uint32_t* tota
         if (total) cuda_check(cudaMemsetAsync(total, 0, sizeof(uint32_t), stream), "memset total");
         return;
     }
-    cuda_check(cudaMemsetAsync(ws.ticket, 0, sizeof(unsigned), stream), "memset ticket");
+    start_tickets(ws, stream);
     const unsigned epoch = ++ws.epoch;
     scan_tiles<0><<<tiles_for(n), kScanBlock, 0, stream>>>(in, nullptr, out, n, total, ws.status, ws.ticket, epoch,
-                                                           ws.err);
+                                                           ws.err, device_wait_limit_ns());
     cuda_check(cudaGetLastError(), "scan launch");
 }
 
@@ -121,10 +147,10 @@ void compact_u32(const uint32_t* values, const uint32_t* flags, uint32_t* out, u
         if (count) cuda_check(cudaMemsetAsync(count, 0, sizeof(uint32_t), stream), "memset count");
         return;
     }
-    cuda_check(cudaMemsetAsync(ws.ticket, 0, sizeof(unsigned), stream), "memset ticket");
+    start_tickets(ws, stream);
     const unsigned epoch = ++ws.epoch;
     scan_tiles<1><<<tiles_for(n), kScanBlock, 0, stream>>>(flags, values, out, n, count, ws.status, ws.ticket, epoch,
-                                                           ws.err);
+                                                           ws.err, device_wait_limit_ns());
     cuda_check(cudaGetLastError(), "compact launch");
 }
 

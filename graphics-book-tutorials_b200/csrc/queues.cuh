@@ -11,8 +11,9 @@
 // [31:0] value. A status written by an earlier scan carries another epoch and reads as "not yet
 // available", so the status array never has to be cleared between scans.
 //
-// Every spin is bounded: a wait that exceeds kSpinLimitNs of %globaltimer sets *err and returns,
-// so a bug can never hang the GPU; callers report the error to the host.
+// Every spin is bounded: a wait that exceeds its limit (kDefaultWaitLimitNs of %globaltimer unless
+// the host set another, device_wait_limit_ns) sets *err and returns, so a bug can never hang the
+// GPU; callers report the error to the host.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -22,7 +23,7 @@ namespace wfb {
 constexpr unsigned kFullMask = 0xffffffffu;
 constexpr unsigned kStatusAggregate = 1u;
 constexpr unsigned kStatusPrefix = 2u;
-constexpr unsigned long long kSpinLimitNs = 2000000000ull;  // 2 s
+constexpr unsigned long long kDefaultWaitLimitNs = 2000000000ull;  // 2 s
 
 #if defined(__CUDACC__)
 
@@ -95,9 +96,9 @@ __device__ __forceinline__ void publish_status(unsigned long long* status, int t
 }
 
 // Exclusive prefix of tile `tile` (> 0) from its predecessors' status words. Called by ONE full
-// warp. Returns the prefix; on a timeout sets *err = 1 and returns 0.
+// warp. Returns the prefix; after waiting longer than limit_ns sets *err = 1 and returns 0.
 __device__ __forceinline__ uint32_t tile_lookback(const unsigned long long* status, int tile, unsigned epoch,
-                                                  unsigned* err) {
+                                                  unsigned* err, unsigned long long limit_ns) {
     const int lane = threadIdx.x & 31;
     const unsigned ep = epoch & 0x3fffffffu;
     uint32_t prefix = 0;
@@ -115,7 +116,7 @@ __device__ __forceinline__ uint32_t tile_lookback(const unsigned long long* stat
             }
             if (__ballot_sync(kFullMask, flag == 0u) == 0) break;
             // warp-uniform timeout decision (lane 0's clock), so all lanes leave together
-            const int late = __shfl_sync(kFullMask, (int)(global_ns() - t0 > kSpinLimitNs), 0);
+            const int late = __shfl_sync(kFullMask, (int)(global_ns() - t0 > limit_ns), 0);
             if (late) {
                 if (lane == 0) atomicExch(err, 1u);
                 return 0;

@@ -270,6 +270,16 @@ void Renderer::configure(int block, int blocks_per_sm, int min_active, int split
     }
 }
 
+void Renderer::set_l2_residency(int mode) {
+    wf_cfg_.l2_persist = mode < 0 ? -1 : (mode > 0 ? 1 : 0);
+    if (mode_ != wf::GpuMode::Wavefront) return;
+    cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+    wf_.reset();
+    wf_ = std::make_unique<Wavefront>(pixels(), wf_cfg_);
+}
+
+uint64_t Renderer::l2_window_bytes() const { return wf_ ? wf_->engine.l2_window_bytes() : 0; }
+
 uint64_t Renderer::device_bytes() const {
     uint64_t b = scene_->bytes + 5ull * pixels() * sizeof(float) + sizeof(DevCounters);
     if (wf_) b += wf_->engine.bytes();

@@ -3,11 +3,12 @@
 //
 //  * Admission: a queued job is admitted when the device bytes of all admitted jobs (film sums +
 //    split-mode sample buffer) stay within the budget and the launch has room.
-//  * Iteration-level scheduling: every launch advances every admitted job by a slice of its
-//    samples; a job that arrives while a launch runs joins the next launch, so new requests
-//    overlap on the device with the ones in progress. The slice is chosen from the measured
+//  * Iteration-level scheduling: every launch advances admitted jobs by slices of their samples;
+//    a job that arrives while a launch runs joins the next launch, so new requests overlap on the
+//    device with the ones in progress. The launch's sample budget comes from the measured
 //    throughput so a launch takes about launch_target_ms, which bounds how long a new arrival
-//    waits before its first samples run.
+//    waits before its first samples run; plan_launch shares it out (express lane for small jobs,
+//    large jobs in arrival order; or equal slices).
 //  * Bit-exactness: slices add samples [done, done + k) to the job's film sums, which is the
 //    progressive API's contract (WVM/include/wf/renderer.hpp:54-60): the finished film equals the
 //    job rendered alone in one call.
@@ -242,25 +243,19 @@ bool Server::admit_locked() {
     return any;
 }
 
-// Samples per job for the next launch: the largest k whose total stays within the launch budget.
-int Server::choose_slice(const std::vector<Job*>& act) {
-    if (cfg_.one_job_per_launch) return 1 << 30;
-    if (cfg_.fixed_slice > 0) return cfg_.fixed_slice;
-    const double budget = msps_estimate_ * 1e3 * cfg_.launch_target_ms;  // samples
-    auto total = [&](int k) {
-        double s = 0.0;
-        for (const Job* j : act)
-            s += (double)j->spec.width * j->spec.height * std::min(k, j->spec.sample_count - j->issued);
-        return s;
-    };
-    int lo = 1, hi = 1;
-    for (const Job* j : act) hi = std::max(hi, j->spec.sample_count - j->issued);
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (total(mid) <= budget) lo = mid;
-        else hi = mid - 1;
+// Samples of each admitted job (in admission order) for the next launch; 0 leaves a job out.
+std::vector<int> Server::plan_launch(const std::vector<Job*>& act) {
+    std::vector<int> k(act.size(), 0);
+    for (size_t i = 0; i < act.size(); ++i) {
+        const int rem = act[i]->spec.sample_count - act[i]->issued;
+        if (cfg_.one_job_per_launch) k[i] = rem;
+        else if (cfg_.fixed_slice > 0) k[i] = std::min(cfg_.fixed_slice, rem);
     }
-    return lo;
+    if (cfg_.one_job_per_launch || cfg_.fixed_slice > 0) return k;
+    std::vector<SliceJob> jobs(act.size());
+    for (size_t i = 0; i < act.size(); ++i)
+        jobs[i] = SliceJob{(double)act[i]->spec.width * act[i]->spec.height, act[i]->spec.sample_count - act[i]->issued};
+    return plan_slices(jobs, msps_estimate_ * 1e3 * cfg_.launch_target_ms, cfg_.schedule);
 }
 
 // Two launches in flight: while the GPU renders launch N, the worker retires launch N-1's
@@ -309,22 +304,30 @@ void Server::worker() {
                 }
         }
         if (!f.jobs.empty()) {
-            // ---- enqueue one launch: every issuable job advances by a slice ----
-            const int k = choose_slice(f.jobs);
+            // ---- enqueue one launch: each planned job advances by its slice ----
+            const std::vector<int> plan = plan_launch(f.jobs);
+            std::vector<Job*> jobs;
+            std::vector<uint64_t> tickets;
             std::vector<JobSpec> specs;
             std::vector<JobBuffers> bufs;
-            for (Job* j : f.jobs) {
+            for (size_t i = 0; i < f.jobs.size(); ++i) {
+                if (plan[i] <= 0) continue;
+                Job* j = f.jobs[i];
                 JobSpec sp = j->spec;
                 sp.first_sample = j->issued;
-                sp.sample_count = std::min(k, j->spec.sample_count - j->issued);
+                sp.sample_count = plan[i];
                 f.samples += (uint64_t)sp.width * sp.height * sp.sample_count;
                 f.counts.push_back(sp.sample_count);
                 JobBuffers b = j->buf;
                 b.chunks = std::min(b.chunks, sp.sample_count);
                 if (b.chunks > 1 && b.lbuf == nullptr) b.chunks = 1;
+                jobs.push_back(j);
+                tickets.push_back(f.tickets[i]);
                 specs.push_back(sp);
                 bufs.push_back(b);
             }
+            f.jobs = std::move(jobs);
+            f.tickets = std::move(tickets);
             f.slot = next_slot;
             next_slot ^= 1;
             try {

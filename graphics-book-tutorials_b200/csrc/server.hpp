@@ -10,6 +10,7 @@
 #include <thread>
 #include <vector>
 #include "batch.hpp"
+#include "schedule.hpp"
 
 namespace wfb {
 
@@ -19,6 +20,7 @@ struct ServerConfig {
     double launch_target_ms = 20.0;       // slice size aims at launches of about this length
     int fixed_slice = 0;                  // > 0: samples per job per launch (0: adaptive)
     bool one_job_per_launch = false;      // plain mode: FIFO, whole job, one launch per job
+    int schedule = kScheduleExpress;      // how a launch's budget is shared (schedule.hpp)
     LaunchConfig launch;  // arm and knobs of every launch
 };
 
@@ -64,7 +66,7 @@ private:
     bool admit_locked();
     void release_idle_locked(bool worker = true);
     void downloader();
-    int choose_slice(const std::vector<Job*>& act);
+    std::vector<int> plan_launch(const std::vector<Job*>& act);
 
     ServerConfig cfg_;
     std::unique_ptr<BatchLauncher> launchers_[2];  // alternate launches: one renders, one is prepared

@@ -24,6 +24,7 @@
 // Stage times come from %globaltimer at the barriers (no host synchronisation).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include "engine.hpp"
 #include "queues.cuh"
 #include "wavefront.hpp"
@@ -61,11 +62,9 @@ struct Pool {
     float4* rad;     // L, depth | specular << 30
     uint2* key;
     int4* unit;      // pixel (-1: none), sample, end sample, 0
-    float4* acc;     // film sums of the unit (direct mode): rgb, lum
+    float4* acc;     // film sums of the unit (direct mode only; outside the pool arena): rgb, lum
     float* acc2;     // lum2
     float4* hit;     // t, prim, u, v
-    float4* surf_p;  // p, material | inside << 31
-    float4* surf_n;  // n
     uint32_t* alive;
     uint32_t* list[2];
     uint32_t* queue[4];  // lambert, metal, dielectric, shadow slots
@@ -85,6 +84,9 @@ struct WfArgs {
     int min_active;
     int leaf_batch;
     int split_shading;  // stage timing: a barrier between material queues
+    unsigned long long wait_ns;  // limit of every bounded wait (grid barriers, look-backs)
+    unsigned bar_extra;          // CTAs a barrier waits for beyond the launch's own (0; 1 only in the
+                                 // wait-timeout test, where no barrier can complete)
 };
 
 // The job a slot's path belongs to (its unit's .w); a single render has only job0.
@@ -124,9 +126,10 @@ __device__ __forceinline__ void store_radiance(const Pool& P, int slot, const wf
     P.rad[slot] = make_float4(ps.L.x, ps.L.y, ps.L.z, __int_as_float(ps.depth | (ps.specular << 30)));
 }
 
-// Grid-wide barrier over co-resident CTAs (cooperative launch). Bounded: a wait longer than
-// kSpinLimitNs, or an error raised elsewhere, makes every CTA leave with `false`.
-__device__ bool grid_sync(Control* c, unsigned nblocks, int stage, unsigned long long* t_last) {
+// Grid-wide barrier over `nblocks` arrivals of co-resident CTAs (cooperative launch). Bounded: a
+// wait longer than limit_ns, or an error raised elsewhere, makes every CTA leave with `false`.
+__device__ bool grid_sync(Control* c, unsigned nblocks, int stage, unsigned long long* t_last,
+                          unsigned long long limit_ns) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -141,7 +144,7 @@ __device__ bool grid_sync(Control* c, unsigned nblocks, int stage, unsigned long
         } else {
             const unsigned long long t0 = global_ns();
             while (*gen == g) {
-                if (*(volatile unsigned*)&c->err != 0u || global_ns() - t0 > kSpinLimitNs) {
+                if (*(volatile unsigned*)&c->err != 0u || global_ns() - t0 > limit_ns) {
                     atomicExch(&c->err, 1u);
                     ok = 0;
                     break;
@@ -261,7 +264,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
     const Pool& P = a.pool;
     Control* c = P.ctl;
     const int lane = threadIdx.x & 31;
-    const unsigned nblocks = gridDim.x;
+    const unsigned nblocks = gridDim.x + a.bar_extra;  // arrivals that complete a barrier
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gthreads = gridDim.x * blockDim.x;
     const unsigned total_units = MULTI ? a.hdr->total_units : a.job0.units;
@@ -383,7 +386,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
             const uint32_t excl = block_exclusive_sum(flag, smem, &agg);
             if (threadIdx.x == 0) publish_status(P.status, tile, iter, tile == 0 ? kStatusPrefix : kStatusAggregate, agg);
             if (tile > 0 && threadIdx.x < 32) {
-                const uint32_t pre = tile_lookback(P.status, tile, iter, &c->err);
+                const uint32_t pre = tile_lookback(P.status, tile, iter, &c->err, a.wait_ns);
                 if (threadIdx.x == 0) {
                     publish_status(P.status, tile, iter, kStatusPrefix, pre + agg);
                     s_prefix = pre;
@@ -397,7 +400,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
             __syncthreads();
         }
         if (ntiles == 0 && gtid == 0) c->n_next = 0;
-        if (!grid_sync(c, nblocks, 6, &t_last)) break;
+        if (!grid_sync(c, nblocks, 6, &t_last, a.wait_ns)) break;
         const unsigned n = *(volatile unsigned*)&c->n_next;
         if (gtid == 0) {
             c->n_active = n;
@@ -408,7 +411,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
 
         // ---------------- E: extension rays ----------------
         traverse_phase<false, MULTI>(a, next, n, &c->fetch[0], &n_ext);
-        if (!grid_sync(c, nblocks, 0, &t_last)) break;
+        if (!grid_sync(c, nblocks, 0, &t_last, a.wait_ns)) break;
 
         // ---------------- C: classify, push material queues ----------------
         for (unsigned base = (unsigned)blockIdx.x * kWfBlock; base < n; base += (unsigned)gthreads) {
@@ -432,13 +435,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                 wf::Surface f;
                 mat = wf::classify(J.s, ps, h, J.max_depth, &f);
                 store_radiance(P, slot, ps);
-                if (mat >= 0) {
-                    P.surf_p[slot] = make_float4(f.p.x, f.p.y, f.p.z,
-                                                 __uint_as_float((unsigned)f.material | ((unsigned)f.inside << 31)));
-                    P.surf_n[slot] = make_float4(f.n.x, f.n.y, f.n.z, 0.0f);
-                } else {
-                    P.alive[slot] = 0u;
-                }
+                if (mat < 0) P.alive[slot] = 0u;
             }
             for (int q = 0; q < 3; ++q) {
                 const bool mine = valid && mat == q;
@@ -446,7 +443,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                 if (mine && at == 0xFFFFFFFFu) P.alive[slot] = 0u;  // dropped on overflow: the path ends
             }
         }
-        if (!grid_sync(c, nblocks, 1, &t_last)) break;
+        if (!grid_sync(c, nblocks, 1, &t_last, a.wait_ns)) break;
 
         // ---------------- S: shade the three material queues ----------------
         unsigned qn[3];
@@ -467,14 +464,14 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                     slot = (int)P.queue[q][i];
                     const DevScene& s = job_at<MULTI>(a, MULTI ? P.unit[slot].w : 0).s;
                     wf::PathState ps = load_path(P, slot);
-                    const float4 sp = P.surf_p[slot], sn = P.surf_n[slot];
-                    wf::Surface f;
-                    f.p = wf::Vec3{sp.x, sp.y, sp.z};
-                    const unsigned mi = __float_as_uint(sp.w);
-                    f.material = (int)(mi & 0x7fffffffu);
-                    f.inside = (int)(mi >> 31);
-                    f.n = wf::Vec3{sn.x, sn.y, sn.z};
-                    f.n_out = f.n;  // not used by the shading steps
+                    // the surface classify saw: make_surface of the same ray and hit, so the same bits
+                    const float4 hv = P.hit[slot];
+                    wf::HitRecord h;
+                    h.t = hv.x;
+                    h.prim = __float_as_int(hv.y);
+                    h.u = hv.z;
+                    h.v = hv.w;
+                    const wf::Surface f = wf::make_surface(s, ps.ray, h);
                     bool alive;
                     if (q == wf::kLambert) {
                         int has = 0;
@@ -496,16 +493,16 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
                     }
                 }
             }
-            if (a.split_shading && !grid_sync(c, nblocks, 2 + q, &t_last)) ok = false;
+            if (a.split_shading && !grid_sync(c, nblocks, 2 + q, &t_last, a.wait_ns)) ok = false;
         }
         if (!ok) break;
-        if (!a.split_shading && !grid_sync(c, nblocks, 2, &t_last)) break;
+        if (!a.split_shading && !grid_sync(c, nblocks, 2, &t_last, a.wait_ns)) break;
 
         // ---------------- H: shadow rays ----------------
         const unsigned nsh = min(*(volatile unsigned*)&c->qcount[3], a.qcap);
         if (gtid == 0 && nsh > c->high_water[3]) c->high_water[3] = nsh;
         traverse_phase<true, MULTI>(a, nullptr, nsh, &c->fetch[1], &n_sh);
-        if (!grid_sync(c, nblocks, 5, &t_last)) break;
+        if (!grid_sync(c, nblocks, 5, &t_last, a.wait_ns)) break;
     }
 
     // ---- fold counters ----
@@ -562,11 +559,9 @@ size_t pool_bytes(int cap, Pool* out, char* base) {
     P.rad = carve<float4>(p, cap);
     P.key = carve<uint2>(p, cap);
     P.unit = carve<int4>(p, cap);
-    P.acc = carve<float4>(p, cap);
-    P.acc2 = carve<float>(p, cap);
+    P.acc = nullptr;  // direct mode only: WavefrontEngine::reserve_direct
+    P.acc2 = nullptr;
     P.hit = carve<float4>(p, cap);
-    P.surf_p = carve<float4>(p, cap);
-    P.surf_n = carve<float4>(p, cap);
     P.alive = carve<uint32_t>(p, cap);
     P.list[0] = carve<uint32_t>(p, cap);
     P.list[1] = carve<uint32_t>(p, cap);
@@ -585,9 +580,44 @@ struct WavefrontEngine::State {
     Pool pool{};
     float* lbuf = nullptr;
     size_t lbuf_floats = 0;
+    void* acc = nullptr;  // direct-mode film sums per slot (float4 + float), allocated on first use
     int grid = 0;        // co-resident CTAs of the single-render kernel
     int grid_multi = 0;  // and of the batch kernel
+    // L2 residency: an access-policy window over the pool arena on every launch (0 bytes: none)
+    size_t window_bytes = 0;
+    float hit_ratio = 0.f;
 };
+
+namespace {
+
+// Persisting-L2 set-aside of this process's context: raised (never lowered) to what the largest
+// L2-resident pool asks for, within the device's maximum. A context resource limit, released with
+// the context; it changes no device setting.
+std::mutex g_l2_mu;
+size_t g_l2_persist = 0;
+
+size_t reserve_persisting_l2(size_t want, int dev) {
+    int max_persist = 0;
+    cuda_check(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev), "persisting L2 size");
+    want = std::min(want, (size_t)std::max(max_persist, 0));
+    std::lock_guard<std::mutex> lock(g_l2_mu);
+    if (want > g_l2_persist) {
+        cuda_check(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want), "persisting L2 set-aside");
+        g_l2_persist = want;
+    }
+    return g_l2_persist;
+}
+
+}  // namespace
+
+size_t wavefront_slot_bytes() { return pool_bytes(1 << 20, nullptr, nullptr) >> 20; }
+
+size_t wavefront_l2_resident_paths(int device) {
+    int max_persist = 0;
+    cuda_check(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, device), "persisting L2 size");
+    const size_t slots = (size_t)std::max(max_persist, 0) / wavefront_slot_bytes();
+    return slots & ~(size_t)(kWfBlock - 1);
+}
 
 WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixels_(pixels), cfg_(cfg) {
     if (pixels <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "wavefront needs at least one pixel");
@@ -602,6 +632,18 @@ WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixel
     pool_bytes(cap, &state_->pool, static_cast<char*>(arena_));
     int dev = 0, sms = 0, occ = 0, coop = 0;
     cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    // L2 residency: the pool (every field a bounce reads or writes) under a persisting window when
+    // it fits the device's persisting set-aside (auto), or whenever asked (a partial window).
+    int max_persist = 0, max_window = 0;
+    cuda_check(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev), "persisting L2 size");
+    cuda_check(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev), "window size");
+    const bool fits = bytes <= (size_t)max_persist;
+    if (max_persist > 0 && max_window > 0 && (cfg.l2_persist > 0 || (cfg.l2_persist < 0 && fits))) {
+        const size_t window = std::min(bytes, (size_t)max_window);
+        const size_t carve = reserve_persisting_l2(window, dev);
+        state_->window_bytes = window;
+        state_->hit_ratio = (float)std::min(1.0, (double)carve / (double)window);
+    }
     cuda_check(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cooperative attribute");
     if (!coop) throw Error(WFB_ERR_UNSUPPORTED, "device does not support cooperative launches");
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
@@ -615,17 +657,33 @@ WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixel
 
 WavefrontEngine::~WavefrontEngine() {
     if (state_ && state_->lbuf) cudaFree(state_->lbuf);
+    if (state_ && state_->acc) cudaFree(state_->acc);
+    if (state_ && state_->window_bytes) cudaCtxResetPersistingL2Cache();  // the pool's lines become normal
     if (arena_) cudaFree(arena_);
 }
 
-uint64_t WavefrontEngine::bytes() const { return bytes_ + (state_ ? state_->lbuf_floats * sizeof(float) : 0); }
+uint64_t WavefrontEngine::bytes() const {
+    if (!state_) return bytes_;
+    return bytes_ + state_->lbuf_floats * sizeof(float) + (state_->acc ? (size_t)capacity_ * 20 : 0);
+}
+
+size_t WavefrontEngine::l2_window_bytes() const { return state_ ? state_->window_bytes : 0; }
+
+void WavefrontEngine::reserve_direct() {
+    State& st = *state_;
+    if (st.acc) return;
+    const size_t acc_bytes = (size_t)capacity_ * sizeof(float4);
+    cuda_check(cudaMalloc(&st.acc, acc_bytes + (size_t)capacity_ * sizeof(float)), "cudaMalloc direct-mode sums");
+    st.pool.acc = static_cast<float4*>(st.acc);
+    st.pool.acc2 = reinterpret_cast<float*>(static_cast<char*>(st.acc) + acc_bytes);
+}
 
 namespace {
 
 // Control reset, pool init, the cooperative launch and the counter fold; returns kernels launched.
 template <bool MULTI>
 int launch_pool(const WfArgs& args, int grid, int capacity, DevCounters* counters, bool count_rays,
-                cudaStream_t stream, KernelTimer* timer = nullptr) {
+                size_t window_bytes, float hit_ratio, cudaStream_t stream, KernelTimer* timer = nullptr) {
     const Pool& pool = args.pool;
     cuda_check(cudaMemsetAsync(pool.ctl, 0, sizeof(Control), stream), "memset control");
     cuda_check(cudaMemsetAsync(pool.status, 0, ((size_t)capacity / kWfBlock + 2) * sizeof(unsigned long long), stream),
@@ -633,11 +691,32 @@ int launch_pool(const WfArgs& args, int grid, int capacity, DevCounters* counter
     wavefront_init<<<(capacity + 255) / 256, 256, 0, stream>>>(pool, capacity);
     cuda_check(cudaGetLastError(), "wavefront init launch");
     WfArgs a = args;
-    void* params[] = {&a};
+    a.wait_ns = device_wait_limit_ns();
+    a.bar_extra = take_unsatisfiable_wait() ? 1u : 0u;
+    // one cooperative launch; the pool arena (it starts at the path-state arrays) under a persisting
+    // L2 window when the engine has one
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    int n_attr = 1;
+    if (window_bytes > 0) {
+        attr[1].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[1].val.accessPolicyWindow.base_ptr = static_cast<void*>(pool.ray_o);
+        attr[1].val.accessPolicyWindow.num_bytes = window_bytes;
+        attr[1].val.accessPolicyWindow.hitRatio = hit_ratio;
+        attr[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        n_attr = 2;
+    }
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(kWfBlock);
+    lc.dynamicSmemBytes = 0;
+    lc.stream = stream;
+    lc.attrs = attr;
+    lc.numAttrs = n_attr;
     if (timer) timer->begin(stream);
-    cuda_check(cudaLaunchCooperativeKernel((const void*)wavefront_persistent<MULTI>, dim3(grid), dim3(kWfBlock), params,
-                                           0, stream),
-               "wavefront cooperative launch");
+    cuda_check(cudaLaunchKernelEx(&lc, wavefront_persistent<MULTI>, a), "wavefront cooperative launch");
     if (timer) timer->end(stream);
     wavefront_fold<<<1, 1, 0, stream>>>(pool.ctl, counters, count_rays ? 1 : 0);
     cuda_check(cudaGetLastError(), "wavefront fold launch");
@@ -677,6 +756,8 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
     if (a.job0.chunks > 1) {
         reserve(film.pixels, p.sample_count);
         a.job0.lbuf = st.lbuf;
+    } else {
+        reserve_direct();
     }
     a.jobs = nullptr;
     a.hdr = nullptr;
@@ -686,7 +767,8 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
     a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = p.stage_timing ? 1 : 0;
-    int launches = launch_pool<false>(a, st.grid, capacity_, counters, p.count_rays, stream, timer);
+    int launches = launch_pool<false>(a, st.grid, capacity_, counters, p.count_rays, st.window_bytes, st.hit_ratio,
+                                      stream, timer);
     if (a.job0.chunks > 1) {
         launch_film_commit(film, a.job0.lbuf, p.sample_count, stream);
         ++launches;
@@ -709,6 +791,7 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
 
 int WavefrontEngine::run_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, DevCounters* counters,
                                bool count_rays, cudaStream_t stream) {
+    reserve_direct();  // a batch may hold direct-mode jobs
     WfArgs a{};
     a.jobs = d_jobs;
     a.hdr = d_hdr;
@@ -718,7 +801,8 @@ int WavefrontEngine::run_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, 
     a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = 0;
-    return launch_pool<true>(a, state_->grid_multi, capacity_, counters, count_rays, stream);
+    return launch_pool<true>(a, state_->grid_multi, capacity_, counters, count_rays, state_->window_bytes,
+                             state_->hit_ratio, stream);
 }
 
 }  // namespace wfb

@@ -28,6 +28,8 @@ public:
                   cudaStream_t stream);
     uint64_t bytes() const;
     int capacity() const { return capacity_; }
+    // Bytes of the pool under a persisting L2 access-policy window on every launch (0: none).
+    size_t l2_window_bytes() const;
 
 private:
     struct State;
@@ -38,6 +40,12 @@ private:
     int pixels_ = 0;
     WavefrontConfig cfg_;
     int chunks_for(int pixels, int sample_count) const;
+    void reserve_direct();  // direct-mode film sums per slot
 };
+
+// Pool bytes per path slot, and the largest pool (a multiple of the block) that fits the
+// device's persisting L2 set-aside.
+size_t wavefront_slot_bytes();
+size_t wavefront_l2_resident_paths(int device);
 
 }  // namespace wfb

@@ -57,6 +57,11 @@ typedef struct {
     int cc_major, cc_minor;
     int sm_count;
     uint64_t total_memory_bytes, free_memory_bytes;
+    /* L2 (no reference counterpart): size, the largest persisting set-aside, the largest
+     * access-policy window, and the largest wavefront pool (paths) that fits the set-aside */
+    uint64_t l2_bytes, persisting_l2_max_bytes, access_window_max_bytes;
+    int wavefront_l2_resident_paths;
+    int wavefront_slot_bytes;
 } wfb_device_facts;
 int wfb_device_facts_get(wfb_device_facts* out);
 
@@ -174,6 +179,14 @@ uint64_t wfb_renderer_device_bytes(wfb_renderer_t r);
  * flight, min_active and leaf_batch. */
 int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int min_active,
                            int split_chunks, int paths_in_flight, int occupancy, int leaf_batch);
+/* Wavefront path pool resident in L2 (no reference counterpart; the reference's pool is W*H paths
+ * in plain device memory, WVM/src/gpu/wavefront.cu:11-26): every wavefront launch carries a
+ * persisting access-policy window over the pool, backed by the context's persisting-L2 set-aside.
+ * mode -1 (default): when the pool fits the device's persisting set-aside; 0: never; 1: always
+ * (a larger pool gets a window with a hit ratio below 1). Megakernel renderers ignore it. */
+int wfb_renderer_set_l2_residency(wfb_renderer_t r, int mode);
+/* Bytes of the wavefront pool under the persisting window (0: none). */
+uint64_t wfb_renderer_l2_window_bytes(wfb_renderer_t r);
 int wfb_renderer_width(wfb_renderer_t r);
 int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */
@@ -246,7 +259,13 @@ typedef struct {
     int fixed_slice;         /* > 0: samples per job per launch */
     int one_job_per_launch;
     wfb_launch_config launch; /* arm and knobs of every launch (split_chunks <= 0: 4 for servers) */
+    int schedule;            /* continuous batching: WFB_SCHEDULE_EXPRESS (0) or WFB_SCHEDULE_SHARED */
 } wfb_server_config;
+/* Schedules: EXPRESS -- jobs whose remaining work fits a quarter of a launch ride in the next launch
+ * whole; large jobs take the rest in arrival order (the oldest always at least a quarter).
+ * SHARED -- every admitted job advances by the same number of samples per launch. */
+#define WFB_SCHEDULE_EXPRESS 0
+#define WFB_SCHEDULE_SHARED 1
 typedef struct {
     uint64_t submitted, completed, cancelled, failed, launches, samples_done;
     double busy_ms, wall_s;
@@ -301,23 +320,36 @@ int wfb_test_queue_push(const uint32_t* d_flags, int n, uint32_t* d_items, uint3
  * (no reference counterpart: the reference's scan has no device-side waits). */
 int wfb_scan_workspace_check(wfb_scan_workspace_t ws, void* stream);
 
+/* Test hook for the bounded device-side waits (no reference counterpart: the reference's GPU arms
+ * have no device-side waits; its failure suite drives the wavefront's error path through
+ * queue_capacity instead, WVM/tests/catch/wavefront_failure.cu:92-114). Sets the limit of every
+ * bounded wait -- wavefront grid barriers and scan look-backs -- to limit_ns for later launches
+ * (0 restores the 2 s default). With unsatisfiable != 0, the NEXT wavefront launch or scan waits
+ * for something that never happens (a barrier expects one CTA more than the launch has; no CTA
+ * claims the first scan tile): its waits run out after limit_ns, the kernel returns, and the call
+ * reports WFB_ERR_DEVICE_WAIT (renders) or wfb_scan_workspace_check does. Process-wide. */
+int wfb_test_bounded_wait(uint64_t limit_ns, int unsatisfiable);
+
 /* ---- allocation-free rendering ---------------------------------------------------------------
  * No counterpart in the reference. For callers that must not allocate device memory on their
- * render path: a host that owns all device memory through its own pool, a real-time loop where
- * an allocation (which can synchronise the device) would break the frame budget, or work issued
- * while a stream is being captured into a CUDA graph (cudaMalloc is not allowed there).
+ * render path: a host that owns all device memory through its own pool and does not let plugins
+ * allocate, or a real-time loop where an allocation (which can synchronise the device) would
+ * break the frame budget.
  *
  * Adds samples [first_sample, first_sample + count) of `scene` -- its own camera and resolution
  * w x h -- to caller-owned DEVICE film sums (rgb_sum 3*w*h floats, lum_sum w*h, lum2_sum w*h),
  * exactly as wfb_renderer_run_passes adds them to a renderer's film (same bits). Enqueued on
- * `stream` (a cudaStream_t; NULL = default stream); the call returns without waiting.
+ * `stream` (a cudaStream_t; NULL = default stream); the call returns without waiting. The scene
+ * may be destroyed as soon as the call returns: its device memory is released only after the
+ * queued work.
  * Allocates nothing: its scratch is one static device array of about 12 MB that every GPU which
  * loads the library holds until the process exits, and that all calls share. Calls that overlap
  * on the GPU therefore race: serialise them (one stream, or wait between calls). The first call
- * on a device looks up the array's address (cudaGetSymbolAddress); make that first call before
- * any stream capture. The scene must already be resident on the current device (creating a
- * renderer on it uploads it). Rejects w * h * count > WFB_NOALLOC_MAX_SAMPLES with
- * WFB_ERR_INVALID_ARGUMENT; render larger requests in passes of fewer samples. */
+ * on a device (and the first after that device's context was reset) looks up the array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. The scene must already
+ * be resident on the current device (creating a renderer on it uploads it). Rejects
+ * w * h * count > WFB_NOALLOC_MAX_SAMPLES with WFB_ERR_INVALID_ARGUMENT; render larger requests
+ * in passes of fewer samples. */
 #define WFB_NOALLOC_MAX_SAMPLES 1048576
 int wfb_render_passes_noalloc(wfb_scene_t scene, int first_sample, int count, uint32_t seed, int max_depth,
                               float* rgb_sum, float* lum_sum, float* lum2_sum, void* stream);

@@ -44,7 +44,7 @@ STRUCTS = [("wfb_scene_desc", "SceneDesc"), ("wfb_scene_info", "SceneInfo"),
            ("wfb_render_params", "_CRenderParams"), ("wfb_render_stats", "_CRenderStats"),
            ("wfb_tune_result", "_CTuneResult"), ("wfb_job_desc", "_CJobDesc"),
            ("wfb_server_config", "_CServerConfig"), ("wfb_server_stats", "_CServerStats"),
-           ("wfb_launch_config", "_CLaunchConfig")]
+           ("wfb_launch_config", "_CLaunchConfig"), ("wfb_device_facts", "_CDeviceFacts")]
 
 
 def test_ctypes_mirrors_match_c_layout(wfb, tmp_path):

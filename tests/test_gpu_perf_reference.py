@@ -63,11 +63,14 @@ def test_faster_than_reference_megakernel_with_equal_image(ref, scene, w, h, spp
         "reference_megakernel_ms": rst["render_ms"], "reference_megakernel_msamples_s": samples / rst["render_ms"] / 1e3,
         "reference_megakernel_wall_s": ref_wall,
     }
-    if scene != "heightfield":  # the reference wavefront needs ~0.5 GB per 1M paths; kept to the two smaller scenes
-        wrgb, _, wst = ref.ref_render_gpu(arrays, 1, spp, 1234, 8)
-        assert np.array_equal(wrgb.view(np.uint32), rrgb.view(np.uint32))
-        result["reference_wavefront_ms"] = wst["render_ms"]
-        result["reference_wavefront_msamples_s"] = samples / wst["render_ms"] / 1e3
+    # the reference wavefront (its pool is W*H paths: about 217 MB at 1280x720)
+    wrgb, wvar, wst = ref.ref_render_gpu(arrays, 1, spp, 1234, 8)
+    assert np.array_equal(wrgb.view(np.uint32), rrgb.view(np.uint32)), "reference wavefront differs"
+    assert np.array_equal(wimg.rgb.view(np.uint32), wrgb.view(np.uint32))
+    assert np.array_equal(wimg.lum_var.view(np.uint32), wvar.view(np.uint32))
+    assert wst["queue_overflows"] == 0 and wst["invalid_hits"] == 0
+    result["reference_wavefront_ms"] = wst["render_ms"]
+    result["reference_wavefront_msamples_s"] = samples / wst["render_ms"] / 1e3
     _record(result)
     assert result["engine_megakernel_msamples_s"] > result["reference_megakernel_msamples_s"]
 
@@ -115,7 +118,34 @@ def test_mixed_job_stream_against_reference_plain_megakernel(ref):
     }
     _record(result)
     # One persistent launch for all 64 jobs against the reference's plain megakernel (one launch per
-    # sample per job). The engine's own one-job-per-launch renders already split every pixel into
-    # one-sample units, so batching them gains little device time; it stays within 10% of them.
-    assert batched_ms < ref_ms / 2.5 and plain_ms < ref_ms / 2.5
+    # sample per job): at least 3x its Msamples/s on the mixed job stream. The engine's own
+    # one-job-per-launch renders already split every pixel into one-sample units, so batching them
+    # gains little device time; it stays within 10% of them.
+    assert batched_ms * 3.0 <= ref_ms, result
+    assert plain_ms * 3.0 <= ref_ms, result
     assert batched_ms < 1.1 * plain_ms
+
+
+@pytest.mark.parametrize("scene", ["icospheres", "heightfield"])
+def test_full_resolution_agrees_with_reference_cpu_arm(ref, scene):
+    """Third correctness criterion at the benchmark resolution: the engine's 1280x720 film against the
+    reference CPU arm (render_cpu, all host threads) at 4 spp, same seed and depth -- at least 99.9%
+    of pixels within 3 combined standard errors (wf::compare_results, WVM/src/film.cpp:45-113; the
+    reference runs the same check at its test size, WVM/tests/test_gpu_render.cu:111-130), no
+    non-finite pixel, no invalid hit and no queue overflow on either engine arm."""
+    wfb = load_engine()
+    w, h, spp = 1280, 720, 4
+    sc = wfb.Scene.generate(scene, w, h, 1234, 16)
+    arrays = sc.export()
+    crgb, cvar, _ = ref.ref_render_cpu(arrays, spp, 1234, 8, 0)
+    cpu = wfb.RenderResult(w, h, spp, crgb, cvar)
+    for mode in (wfb.MEGAKERNEL, wfb.WAVEFRONT):
+        r = wfb.GpuRenderer(sc, mode)
+        st = wfb.RenderStats()
+        out = r.render(wfb.RenderParams(spp=spp, seed=1234, max_depth=8), st)
+        r.close()
+        d = wfb.compare_results(cpu, out)
+        _record({"scene": scene, "size": f"{w}x{h}", "spp": spp, "arm": int(mode), "vs_reference_cpu": d})
+        assert d["frac_within_3se"] >= 0.999, d
+        assert d["nonfinite"] == 0 and np.isfinite(out.lum_var).all()
+        assert st.invalid_hits == 0 and st.queue_overflows == 0

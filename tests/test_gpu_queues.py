@@ -125,3 +125,29 @@ def test_queue_push_multiset_and_overflow(wfb, ref, torch, pattern, capacity):
         assert (got[capacity:] == CANARY).all() if capacity else (got == CANARY).all()
         kept = np.sort(got[:stored])
         assert len(np.unique(kept)) == stored and np.isin(kept, want).all(), impl
+
+
+def test_a_look_back_that_cannot_complete_gives_up(wfb, torch):
+    """The next scan claims tiles from 1 on, so no tile publishes the first prefix and every look-back
+    waits for it; with a 1 ms limit the waits give up, the kernel returns, the workspace reports
+    WFB_ERR_DEVICE_WAIT, and a scan on a fresh workspace is exact."""
+    n = 100000
+    x = np.arange(n, dtype=np.uint32) % 7
+    want = np.concatenate([np.zeros(1, np.uint64), np.cumsum(x, dtype=np.uint64)[:-1]]).astype(np.uint32)
+    ws = wfb.ScanWorkspace(n)
+    d = dev(torch, x)
+    out = dev(torch, np.zeros(n, np.uint32))
+    try:
+        wfb.set_bounded_wait_test(1_000_000, unsatisfiable=True)
+        assert ws.scan_exclusive_u32(d.data_ptr(), out.data_ptr(), n) == 0
+        torch.cuda.synchronize()
+    finally:
+        wfb.set_bounded_wait_test(0)
+    with pytest.raises(wfb.WfbError) as e:
+        ws.check()
+    assert e.value.status == wfb.ERR_DEVICE_WAIT
+    ws2 = wfb.ScanWorkspace(n)
+    assert ws2.scan_exclusive_u32(d.data_ptr(), out.data_ptr(), n) == 0
+    torch.cuda.synchronize()
+    ws2.check()
+    assert np.array_equal(host(out), want)

@@ -126,3 +126,30 @@ def test_depth_zero_and_deep_paths(wfb, ref):
         out, _, _ = render(wfb, wfb.Scene.from_arrays(arrays), wfb.WAVEFRONT, 2, 7, depth)
         rrgb, _, _ = ref.ref_render_gpu(arrays, 0, 2, 7, depth)
         assert np.array_equal(bits(out.rgb), bits(rrgb)), depth
+
+
+def test_a_grid_barrier_that_cannot_complete_gives_up_and_the_next_render_is_exact(wfb):
+    """Bounded device-side waits: the next launch's grid barriers wait for one CTA more than the launch
+    has (nothing can complete them); with a 1 ms limit every CTA gives up, the kernel returns, the
+    render reports WFB_ERR_DEVICE_WAIT, and the same renderer's next render is bit-exact (the
+    reference's failure suite checks the same recovery after its queue overflows,
+    WVM/tests/catch/wavefront_failure.cu:92-114)."""
+    import time
+    scene = wfb.Scene.generate("icospheres", 64, 36, 1234, 16)
+    mk, _, _ = render(wfb, scene, wfb.MEGAKERNEL, 4, 5, 8)
+    r = wfb.GpuRenderer(scene, wfb.WAVEFRONT)
+    params = wfb.RenderParams(spp=4, seed=5, max_depth=8)
+    assert np.array_equal(bits(r.render(params).rgb), bits(mk.rgb))
+    try:
+        wfb.set_bounded_wait_test(1_000_000, unsatisfiable=True)
+        t0 = time.perf_counter()
+        with pytest.raises(wfb.WfbError) as e:
+            r.render(params)
+        waited = time.perf_counter() - t0
+    finally:
+        wfb.set_bounded_wait_test(0)
+    assert e.value.status == wfb.ERR_DEVICE_WAIT
+    assert waited < 1.5, f"the failed render took {waited:.3f} s"
+    again = r.render(params)
+    assert np.array_equal(bits(again.rgb), bits(mk.rgb))
+    assert np.array_equal(bits(again.lum_var), bits(mk.lum_var))

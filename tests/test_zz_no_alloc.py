@@ -1,6 +1,6 @@
 """wfb_render_passes_noalloc: the render entry point for callers that cannot allocate device memory
-(a host that owns all device memory through its own pool, a real-time loop, work issued under CUDA
-graph capture). The test owns the film buffers (allocated here with torch, as such a caller's pool
+(a host that owns all device memory through its own pool, or a real-time loop where an allocation
+would break the frame budget). The test owns the film buffers (allocated here with torch, as such a caller's pool
 would), calls the entry point through the C ABI and checks the film against the renderer's, bit for
 bit -- the tolerance every film test in this suite uses -- on two calls in a row."""
 import ctypes
@@ -95,3 +95,30 @@ def test_noalloc_rejects_oversize_and_non_resident_scene(wfb):
     with pytest.raises(wfb.WfbError, match="WFB_NOALLOC_MAX_SAMPLES") as e:
         _call(wfb, fn, scene, 0, 1048576 // (64 * 36) + 1, 1, 8, film)
     assert e.value.status == wfb.ERR_INVALID_ARGUMENT
+
+
+def test_noalloc_on_a_non_blocking_stream_with_the_scene_destroyed_at_once(wfb):
+    """The call returns without waiting; the caller may destroy the scene right away. The scene's
+    device memory must outlive the queued render, which runs on a stream that the library's own
+    (legacy default) stream does not wait for."""
+    torch = pytest.importorskip("torch")
+    fn = _noalloc(wfb)
+    w, h = 1280, 720  # 921,600 samples: one call of the largest size the scratch array takes
+    scene = wfb.Scene.generate("icospheres", w, h, 1234, 16)
+    keep, want = _expected(wfb, scene, 2, 1, 99, 8)
+    film = _film(torch, w, h)
+    stream = torch.cuda.Stream()  # created with cudaStreamNonBlocking
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        st = fn(scene.handle, 2, 1, 99, 8, film[0].data_ptr(), film[1].data_ptr(), film[2].data_ptr(),
+                ctypes.c_void_p(stream.cuda_stream))
+    assert st == wfb.OK, wfb.load_library().wfb_last_error().decode()
+    keep.close()
+    scene.close()  # last owner gone: the arena release is queued behind the render
+    # an identical scene uploaded at once may take the released memory from the same pool
+    again = wfb.Scene.generate("icospheres", w, h, 1234, 16)
+    keep_again = wfb.GpuRenderer(again, wfb.MEGAKERNEL)
+    stream.synchronize()
+    for got, exp in zip(film, want):
+        assert np.array_equal(_bits(got.cpu().numpy()), _bits(exp))
+    keep_again.close()
