@@ -3,11 +3,14 @@
 // 12+ kernels per bounce and synchronises the host 3 times per bounce.
 //
 // Path pool: `capacity` slots, structure of arrays (one array per field, coalesced by slot id),
-// sized by paths_in_flight so that the pool can stay L2-resident. A slot owns a work unit (a pixel
-// and a run of its samples, as in the megakernel) and, when its path ends, regenerates the next
-// sample of the same pixel or takes a new unit: paths in flight stay constant until the work runs
-// out. Film sums are kept per slot in sample order (direct mode) or per (pixel, sample) in a
-// buffer committed in order afterwards (split mode), so the film is bit-identical to every arm.
+// in one arena. A pool that fits the device's persisting L2 set-aside (about 180 B per slot, so a
+// few hundred thousand paths on a B200; wavefront_l2_resident_paths) runs under a persisting
+// access-policy window on every launch, so its state stays in L2 across bounces; larger pools (up
+// to 8M paths) stream through HBM. A slot owns a work unit (a pixel and a run of its samples, as in
+// the megakernel) and, when its path ends, regenerates the next sample of the same pixel or takes a
+// new unit: paths in flight stay constant until the work runs out. Film sums are kept per slot in
+// sample order (direct mode) or per (pixel, sample) in a buffer committed in order afterwards
+// (split mode), so the film is bit-identical to every arm.
 //
 // One bounce = five phases separated by grid barriers (bounded spins, error flag on timeout):
 //   R  regenerate + compact: ended slots commit their sample and start the next one (or fetch a

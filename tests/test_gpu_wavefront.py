@@ -153,3 +153,34 @@ def test_a_grid_barrier_that_cannot_complete_gives_up_and_the_next_render_is_exa
     again = r.render(params)
     assert np.array_equal(bits(again.rgb), bits(mk.rgb))
     assert np.array_equal(bits(again.lum_var), bits(mk.lum_var))
+
+
+def test_l2_resident_pool_renders_the_same_film(wfb):
+    """The largest pool that fits the device's persisting L2 set-aside runs under a persisting
+    access-policy window; with or without the window, and against the megakernel, the film is
+    bit-identical (residency is a cache policy, never a change of arithmetic)."""
+    facts = wfb.device_facts()
+    assert facts["l2_bytes"] > 0 and facts["wavefront_slot_bytes"] > 0
+    paths = facts["wavefront_l2_resident_paths"]
+    if facts["persisting_l2_max_bytes"] == 0 or paths < 1024:
+        pytest.skip("no persisting L2 set-aside on this device")
+    assert paths * facts["wavefront_slot_bytes"] <= facts["persisting_l2_max_bytes"]
+    scene = wfb.Scene.generate("icospheres", 320, 180, 1234, 16)
+    mk, _, _ = render(wfb, scene, wfb.MEGAKERNEL, 8, 9, 8)
+    r = wfb.GpuRenderer(scene, wfb.WAVEFRONT)
+    r.configure(paths_in_flight=paths)
+    assert r.l2_window_bytes() > 0, "a pool that fits the set-aside gets a window by default"
+    params = wfb.RenderParams(spp=8, seed=9, max_depth=8)
+    st = wfb.RenderStats()
+    out = r.render(params, st)
+    assert np.array_equal(bits(out.rgb), bits(mk.rgb)) and np.array_equal(bits(out.lum_var), bits(mk.lum_var))
+    assert st.queue_overflows == 0 and st.invalid_hits == 0
+    r.set_l2_residency(0)
+    assert r.l2_window_bytes() == 0
+    assert np.array_equal(bits(r.render(params).rgb), bits(mk.rgb))
+    big = wfb.GpuRenderer(scene, wfb.WAVEFRONT)
+    big.configure(paths_in_flight=1 << 22)
+    assert big.l2_window_bytes() == 0, "a pool above the set-aside gets no window unless asked"
+    big.set_l2_residency(1)
+    assert big.l2_window_bytes() > 0
+    assert np.array_equal(bits(big.render(params).rgb), bits(mk.rgb))
