@@ -345,6 +345,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--size", default=None, help="WxH override (profiling cases only; not a bench line)")
     ap.add_argument("--spp", type=int, default=None, help="spp override (profiling cases only)")
+    ap.add_argument("--scene", default=None, choices=["icospheres", "heightfield", "cornell36"],
+                    help="scene override (profiling cases only; the bench line is icospheres)")
     ap.add_argument("--mode", default="render", choices=["render", "batch", "serve"],
                     help="render: the icospheres 1280x720 64-spp line; batch: the 64-job mix; serve: a sweep of arrival rates")
     ap.add_argument("--lambdas", default="5,10,20,50,100,200")
@@ -362,12 +364,14 @@ def main():
     elif args.gpus > 1:
         sys.exit(launch_ranks(args.gpus, sys.argv[1:]))
     args.warmup = max(args.warmup, 3)
-    global WIDTH, HEIGHT, SPP, WORKLOAD
+    global WIDTH, HEIGHT, SPP, WORKLOAD, SCENE
     if args.size:
         WIDTH, HEIGHT = (int(v) for v in args.size.lower().split("x"))
     if args.spp:
         SPP = args.spp
-    WORKLOAD = f"{SCENE}-512 {WIDTH}x{HEIGHT} {SPP}spp depth{DEPTH} seed{SEED}"
+    if args.scene:
+        SCENE = args.scene
+    WORKLOAD = f"{SCENE}{'-512' if SCENE == 'icospheres' else ''} {WIDTH}x{HEIGHT} {SPP}spp depth{DEPTH} seed{SEED}"
     if args.impl == "reference":
         run_reference(args)
         return
