@@ -107,7 +107,7 @@ class _CTuneResult(ctypes.Structure):
                 ("wf_min_active", ctypes.c_int),
                 ("msamples_s", ctypes.c_double),
                 ("megakernel_msamples_s", ctypes.c_double), ("wavefront_msamples_s", ctypes.c_double),
-                ("candidates", ctypes.c_int)]
+                ("candidates", ctypes.c_int), ("wf_occupancy", ctypes.c_int)]
 
 
 @dataclass
@@ -460,13 +460,15 @@ class TuneResult:
     megakernel_msamples_s: float
     wavefront_msamples_s: float
     candidates: int
+    wf_occupancy: int
     _c: _CTuneResult = field(repr=False, default=None)
 
     def as_dict(self) -> dict:
         return {"arm": "megakernel" if self.mode == MEGAKERNEL else "wavefront",
                 "megakernel": {"block": self.block, "occupancy": self.occupancy, "min_active": self.min_active,
                                "leaf_batch": self.leaf_batch},
-                "wavefront": {"paths_in_flight": self.paths_in_flight, "min_active": self.wf_min_active},
+                "wavefront": {"paths_in_flight": self.paths_in_flight, "min_active": self.wf_min_active,
+                              "occupancy": self.wf_occupancy},
                 "msamples_s": round(self.msamples_s, 2),
                 "megakernel_msamples_s": round(self.megakernel_msamples_s, 2),
                 "wavefront_msamples_s": round(self.wavefront_msamples_s, 2), "candidates": self.candidates}
@@ -481,7 +483,7 @@ def autotune(scene: Scene, width: int, height: int, probe_spp: int = 2, max_dept
                                        1 if try_wavefront else 0, ctypes.byref(c)))
     return TuneResult(c.mode, c.block, c.occupancy, c.min_active, c.leaf_batch, c.paths_in_flight, c.wf_min_active,
                       c.msamples_s,
-                      c.megakernel_msamples_s, c.wavefront_msamples_s, c.candidates, c)
+                      c.megakernel_msamples_s, c.wavefront_msamples_s, c.candidates, c.wf_occupancy, c)
 
 
 def compare_results(a: RenderResult, b: RenderResult) -> dict:

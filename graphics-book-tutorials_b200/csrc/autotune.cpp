@@ -10,9 +10,11 @@
 //   megakernel: stage 1, (block, occupancy target) in {(128,10), (128,8), (128,6), (128,0), (64,0), (256,0)}
 //               x min_active in {8, 16, 24} at leaf_batch 8; stage 2, the stage-1 winner with
 //               leaf_batch in {4, 12, 16, 32}
-//   wavefront:  paths in flight in {the largest pool that fits the persisting L2 set-aside (its
-//               launches carry a persisting access-policy window), 1M, 2M, 4M, 8M} x min_active
-//               {16, 24}, probed with at least 8 samples so that the pool can fill. Queue capacity is
+//   wavefront:  stage 1, paths in flight in {the largest pool that fits the persisting L2 set-aside
+//               (its launches carry a persisting access-policy window), 2M, 4M, 8M} (each capped at 64
+//               per pixel, duplicates probed once) x register cap {10, 8} CTAs per SM; stage 2,
+//               min_active {16, 24}; probed with enough samples that the largest pool turns over about
+//               twice (8 to 64 per pixel). Queue capacity is
 //               not a knob: every queue is sized to the pool, so none can drop a path (the
 //               reference's capacity knob exists to test overflow, WVM/src/gpu/wavefront.cu:279-280).
 #include <algorithm>
@@ -98,26 +100,46 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
     if (try_wavefront) {
         int dev = 0;
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        const long long pixels = (long long)width * height;
+        // effective pool sizes (the engine caps a pool at 64 slots per pixel), each probed once
+        std::vector<int> pools;
         const int l2_pool = (int)wavefront_l2_resident_paths(dev);
-        std::vector<int> pools = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
-        if (l2_pool >= 1 << 16) pools.insert(pools.begin(), l2_pool);
-        const int actives[] = {16, 24};
-        PassParams pw = p;  // enough samples for the larger pools to fill
-        pw.sample_count = std::max(probe_spp, 8);
+        for (long long want : {(long long)l2_pool, 1ll << 21, 1ll << 22, 1ll << 23}) {
+            if (want < (1 << 16)) continue;
+            const int eff = (int)std::max<long long>(32, std::min(want, 64 * pixels));
+            if (std::find(pools.begin(), pools.end(), eff) == pools.end()) pools.push_back(eff);
+        }
+        // probes long enough that the largest pool turns over about twice (at least 8 samples)
+        PassParams pw = p;
+        const long long fill = 2ll * *std::max_element(pools.begin(), pools.end());
+        pw.sample_count = (int)std::min<long long>(64, std::max<long long>({(long long)probe_spp, 8ll,
+                                                                             (fill + pixels - 1) / pixels}));
         const double samples_w = (double)width * height * pw.sample_count;
         Renderer r(scene, wf::GpuMode::Wavefront);
         r.set_camera(cam, width, height);
+        // stage 1: pool x register cap at the default min_active; stage 2: min_active
+        const int occs[] = {10, 8};
         for (int pool : pools)
-            for (int ma : actives) {
-                r.configure(-1, -1, ma, -1, pool, -1);
+            for (int occ : occs) {
+                r.configure(-1, -1, -1, -1, pool, occ);
                 const double ms = measure(r, pw) * samples / samples_w;  // per probe_spp samples
                 best.candidates++;
                 if (ms < wf_ms) {
                     wf_ms = ms;
                     best.paths_in_flight = pool;
-                    best.wf_min_active = ma;
+                    best.wf_occupancy = occ;
                 }
             }
+        best.wf_min_active = WavefrontConfig{}.min_active;
+        for (int ma : {16, 24}) {
+            r.configure(-1, -1, ma, -1, best.paths_in_flight, best.wf_occupancy);
+            const double ms = measure(r, pw) * samples / samples_w;
+            best.candidates++;
+            if (ms < wf_ms) {
+                wf_ms = ms;
+                best.wf_min_active = ma;
+            }
+        }
     }
     best.megakernel_msamples_s = samples / mk_ms / 1e3;
     if (try_wavefront) best.wavefront_msamples_s = samples / wf_ms / 1e3;
@@ -134,7 +156,7 @@ void apply_tuning(Renderer& r, const TuneResult& t) {
                     t.occupancy >= 0 ? t.occupancy : -1, t.leaf_batch > 0 ? t.leaf_batch : -1);
     else
         r.configure(-1, -1, t.wf_min_active > 0 ? t.wf_min_active : -1, -1,
-                    t.paths_in_flight > 0 ? t.paths_in_flight : -1, -1);
+                    t.paths_in_flight > 0 ? t.paths_in_flight : -1, t.wf_occupancy >= 0 ? t.wf_occupancy : -1);
 }
 
 }  // namespace wfb

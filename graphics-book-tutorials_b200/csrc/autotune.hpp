@@ -10,7 +10,7 @@ struct TuneResult {
     // Best megakernel knobs.
     int block = 128, occupancy = 0, min_active = 16, leaf_batch = 8;
     // Best wavefront knobs (0: not tried, library defaults).
-    int paths_in_flight = 0, wf_min_active = 0;
+    int paths_in_flight = 0, wf_min_active = 0, wf_occupancy = -1;
     double msamples_s = 0.0;             // the winner's measured rate
     double megakernel_msamples_s = 0.0;  // best megakernel candidate
     double wavefront_msamples_s = 0.0;   // best wavefront candidate (0 if not tried)

@@ -135,7 +135,7 @@ wfb::LaunchConfig launch_config(const wfb_launch_config* c) {
     l.use_graph = c->use_graph != 0;
     if (c->block > 0) l.mk.block = c->block;
     need(l.mk.block == 64 || l.mk.block == 128 || l.mk.block == 256, "block must be 64, 128 or 256");
-    if (c->occupancy >= 0) l.mk.occupancy = c->occupancy;
+    if (c->occupancy >= 0) l.mk.occupancy = l.wf.occupancy = c->occupancy;
     else if (l.mk.block != 128) l.mk.occupancy = 0;  // the register-cap targets exist for block 128 only
     need(l.mk.occupancy == 0 || (occupancy_target(l.mk.occupancy) && l.mk.block == 128),
          "occupancy target must be 0, 6, 8 or 10 (block 128)");
@@ -450,6 +450,7 @@ int wfb_autotune(wfb_scene_t scene, int width, int height, int probe_spp, int ma
         out->leaf_batch = t.leaf_batch;
         out->paths_in_flight = t.paths_in_flight;
         out->wf_min_active = t.wf_min_active;
+        out->wf_occupancy = t.wf_occupancy;
         out->msamples_s = t.msamples_s;
         out->megakernel_msamples_s = t.megakernel_msamples_s;
         out->wavefront_msamples_s = t.wavefront_msamples_s;
@@ -468,6 +469,7 @@ int wfb_renderer_apply_tuning(wfb_renderer_t r, const wfb_tune_result* t) {
         tr.leaf_batch = t->leaf_batch;
         tr.paths_in_flight = t->paths_in_flight;
         tr.wf_min_active = t->wf_min_active;
+        tr.wf_occupancy = t->wf_occupancy;
         wfb::apply_tuning(*r->r, tr);
     });
 }

@@ -260,8 +260,9 @@ void Renderer::configure(int block, int blocks_per_sm, int min_active, int split
     if (split_chunks >= 0) mk_cfg_.split_chunks = split_chunks;
     if (occupancy >= 0) mk_cfg_.occupancy = occupancy;
     if (leaf_batch > 0) mk_cfg_.leaf_batch = leaf_batch;
-    if (mode_ == wf::GpuMode::Wavefront && (paths_in_flight > 0 || min_active > 0 || leaf_batch > 0)) {
+    if (mode_ == wf::GpuMode::Wavefront && (paths_in_flight > 0 || min_active > 0 || leaf_batch > 0 || occupancy >= 0)) {
         if (paths_in_flight > 0) wf_cfg_.paths_in_flight = paths_in_flight;
+        if (occupancy >= 0) wf_cfg_.occupancy = occupancy;
         if (min_active > 0) wf_cfg_.min_active = min_active;
         if (leaf_batch > 0) wf_cfg_.leaf_batch = leaf_batch;
         cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");

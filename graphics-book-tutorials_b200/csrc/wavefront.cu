@@ -37,7 +37,7 @@ namespace wfb {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kWfBlock = 256;
+constexpr int kWfBlock = 128;
 constexpr int kStages = 8;  // extend, classify, lambert, metal, dielectric, shadow, compact, other
 
 struct Control {
@@ -49,6 +49,8 @@ struct Control {
     unsigned fetch[2];   // extend, shadow dynamic-fetch cursors
     unsigned unit_next;
     unsigned ticket;
+    unsigned retired;    // extension rays finished in the current E phase
+    unsigned suspended;  // extension rays carried over to the next iteration (all phases)
     unsigned err;
     unsigned overflow;
     unsigned invalid;
@@ -67,8 +69,9 @@ struct Pool {
     int4* unit;      // pixel (-1: none), sample, end sample, 0
     float4* acc;     // film sums of the unit (direct mode only; outside the pool arena): rgb, lum
     float* acc2;     // lum2
-    float4* hit;     // t, prim, u, v
-    uint32_t* alive;
+    float4* hit;     // t, prim, u, v (a suspended ray: its best hit so far)
+    int2* trav;      // a suspended ray's traversal state: next node, pending leaf
+    uint32_t* alive;  // 0: no path, 1: path with a ray to trace, 2: extension ray suspended mid-traversal
     uint32_t* list[2];
     uint32_t* queue[4];  // lambert, metal, dielectric, shadow slots
     float4* sh_dir;      // shadow records: direction, tmax
@@ -87,6 +90,7 @@ struct WfArgs {
     int min_active;
     int leaf_batch;
     int split_shading;  // stage timing: a barrier between material queues
+    int suspend;        // extension stragglers may be suspended to the next iteration
     unsigned long long wait_ns;  // limit of every bounded wait (grid barriers, look-backs)
     unsigned bar_extra;          // CTAs a barrier waits for beyond the launch's own (0; 1 only in the
                                  // wait-timeout test, where no barrier can complete)
@@ -170,9 +174,17 @@ __device__ bool grid_sync(Control* c, unsigned nblocks, int stage, unsigned long
 
 // Resumable closest-hit / any-hit traversal over a list of rays fetched dynamically.
 // Extend: items[i] are slot ids. Shadow: the rays are shadow records 0..n-1 (items unused).
+//
+// Extension stragglers: the phase ends when its last ray does, and near the end a few long rays
+// keep whole warps (and the grid barrier) waiting. Once `suspend_at` of the phase's n rays have
+// finished, a warp that has nothing left to fetch parks its unfinished rays instead -- next node,
+// pending leaf and best hit into the pool, slot state 2 -- and leaves; the slot skips this bounce's
+// classify and shading, stays in the active list, and its ray resumes from exactly that state in
+// the next iteration's extend phase. The traversal steps are the same, so the hit is the same.
 template <bool SHADOW, bool MULTI>
 __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned n, unsigned* cursor,
-                               unsigned long long* n_rays) {
+                               unsigned long long* n_rays, unsigned* retired = nullptr,
+                               unsigned suspend_at = 0xffffffffu) {
     const Pool& P = a.pool;
     // BVH of the lane's current ray: a batch reads its job's from the table at fetch time
     const float4* nodes = a.job0.s.nodes;
@@ -218,6 +230,17 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
                     o = wf::Vec3{oo.x, oo.y, oo.z};
                     traversal_begin(n_nodes, wf::Vec3{d.x, d.y, d.z}, d.w, &ray, &node, &h);
                     pend = 0;
+                    if (!SHADOW && P.alive[slot] == 2u) {  // resume a suspended ray where it stopped
+                        const int2 tv = P.trav[slot];
+                        const float4 hv = P.hit[slot];
+                        node = tv.x;
+                        pend = tv.y;
+                        h.t = hv.x;
+                        h.prim = __float_as_int(hv.y);
+                        h.u = hv.z;
+                        h.v = hv.w;
+                        P.alive[slot] = 1u;
+                    }
                 } else {
                     exhausted = true;
                 }
@@ -226,6 +249,7 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
         if (__ballot_sync(kFull, item >= 0) == 0) return;
         // rounds of box steps or primitive steps while enough lanes traverse (or nothing is left
         // to fetch); see box_step / prim_step
+        unsigned round = 0;
         for (;;) {
             const bool in_leaf = pend != 0;
             const bool at_box = node >= 0 && !in_leaf;
@@ -234,6 +258,25 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
             const unsigned tm = pm | bm;
             if (tm == 0) break;
             if (__popc(tm) < a.min_active && __ballot_sync(kFull, !(in_leaf || at_box) && !exhausted) != 0) break;
+            if (!SHADOW && (++round & 31u) == 0u && __ballot_sync(kFull, exhausted) != 0) {
+                // nothing left to fetch: suspend the warp's rays once most of the phase is done
+                unsigned done = 0;
+                if (lane == 0) done = *(volatile unsigned*)retired;
+                done = __shfl_sync(kFull, done, 0);
+                if (done >= suspend_at) {
+                    const unsigned sm = __ballot_sync(kFull, item >= 0);
+                    if (item >= 0) {
+                        P.trav[id] = make_int2(node, pend);
+                        P.hit[id] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
+                        P.alive[id] = 2u;
+                        item = -1;
+                        node = -1;
+                        pend = 0;
+                    }
+                    if (lane == 0) atomicAdd(&a.pool.ctl->suspended, (unsigned)__popc(sm));
+                    return;
+                }
+            }
             const int np = __popc(pm);
             if (np != 0 && (np >= a.leaf_batch || np >= __popc(bm))) {
                 if (in_leaf) prim_step(prims, n_spheres, o, ray, SHADOW, node, pend, h);
@@ -242,7 +285,12 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
             }
         }
         // retire finished rays
-        if (item >= 0 && node < 0 && pend == 0) {
+        const bool fin = item >= 0 && node < 0 && pend == 0;
+        if (!SHADOW) {
+            const unsigned fm = __ballot_sync(kFull, fin);
+            if (fm && lane == __ffs(fm) - 1) atomicAdd(retired, (unsigned)__popc(fm));
+        }
+        if (fin) {
             ++*n_rays;
             if (SHADOW) {
                 if (h.prim < 0) {  // unoccluded: L += contrib
@@ -262,8 +310,11 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
     }
 }
 
-template <bool MULTI>
-__global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a) {
+// MINB > 1 caps registers so that MINB CTAs fit an SM (the whole bounce loop is one kernel, so its
+// register count is the largest of any phase's; the traversal phases want the warps more than the
+// shading phases want the registers).
+template <bool MULTI, int MINB>
+__global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfArgs a) {
     const Pool& P = a.pool;
     Control* c = P.ctl;
     const int lane = threadIdx.x & 31;
@@ -290,6 +341,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
         if (gtid == 0) {
             c->qcount[0] = c->qcount[1] = c->qcount[2] = c->qcount[3] = 0;
             c->fetch[0] = c->fetch[1] = 0;
+            c->retired = 0;
         }
         const unsigned ntiles = (n_act + kWfBlock - 1) / kWfBlock;
         for (;;) {
@@ -413,7 +465,9 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
         if (n == 0) break;
 
         // ---------------- E: extension rays ----------------
-        traverse_phase<false, MULTI>(a, next, n, &c->fetch[0], &n_ext);
+        // stragglers may be suspended once 95% of a large phase's rays have finished
+        traverse_phase<false, MULTI>(a, next, n, &c->fetch[0], &n_ext, &c->retired,
+                                     a.suspend && n >= 4096 ? n - n / 20 : 0xffffffffu);
         if (!grid_sync(c, nblocks, 0, &t_last, a.wait_ns)) break;
 
         // ---------------- C: classify, push material queues ----------------
@@ -422,7 +476,7 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
             const bool valid = i < n;
             const int slot = valid ? (int)next[i] : 0;
             int mat = -1;
-            if (valid) {
+            if (valid && P.alive[slot] != 2u) {  // a suspended ray has no hit yet
                 const float4 hv = P.hit[slot];
                 wf::HitRecord h;
                 h.t = hv.x;
@@ -521,6 +575,19 @@ __global__ void __launch_bounds__(kWfBlock) wavefront_persistent(const WfArgs a)
     }
 }
 
+using WfKernel = void (*)(const WfArgs);
+
+// The compiled register-cap variants: 0 (none), 6, 8 or 10 CTAs of kWfBlock threads per SM.
+template <bool MULTI>
+WfKernel wavefront_kernel(int occupancy) {
+    switch (occupancy) {
+        case 6: return wavefront_persistent<MULTI, 6>;
+        case 8: return wavefront_persistent<MULTI, 8>;
+        case 10: return wavefront_persistent<MULTI, 10>;
+        default: return wavefront_persistent<MULTI, 1>;
+    }
+}
+
 __global__ void wavefront_init(Pool P, int capacity) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
@@ -565,6 +632,7 @@ size_t pool_bytes(int cap, Pool* out, char* base) {
     P.acc = nullptr;  // direct mode only: WavefrontEngine::reserve_direct
     P.acc2 = nullptr;
     P.hit = carve<float4>(p, cap);
+    P.trav = carve<int2>(p, cap);
     P.alive = carve<uint32_t>(p, cap);
     P.list[0] = carve<uint32_t>(p, cap);
     P.list[1] = carve<uint32_t>(p, cap);
@@ -584,6 +652,7 @@ struct WavefrontEngine::State {
     float* lbuf = nullptr;
     size_t lbuf_floats = 0;
     void* acc = nullptr;  // direct-mode film sums per slot (float4 + float), allocated on first use
+    WfKernel kernel = nullptr, kernel_multi = nullptr;  // the register-cap variant of cfg.occupancy
     int grid = 0;        // co-resident CTAs of the single-render kernel
     int grid_multi = 0;  // and of the batch kernel
     // L2 residency: an access-policy window over the pool arena on every launch (0 bytes: none)
@@ -624,7 +693,7 @@ size_t wavefront_l2_resident_paths(int device) {
 
 WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixels_(pixels), cfg_(cfg) {
     if (pixels <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "wavefront needs at least one pixel");
-    int cap = cfg.paths_in_flight > 0 ? cfg.paths_in_flight : (1 << 22);
+    int cap = cfg.paths_in_flight > 0 ? cfg.paths_in_flight : (1 << 23);
     if (cap > pixels * 64) cap = pixels * 64;  // never more slots than units can use
     if (cap < 32) cap = 32;
     capacity_ = cap;
@@ -650,10 +719,14 @@ WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixel
     cuda_check(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cooperative attribute");
     if (!coop) throw Error(WFB_ERR_UNSUPPORTED, "device does not support cooperative launches");
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wavefront_persistent<false>, kWfBlock, 0), "occupancy");
+    if (cfg.occupancy != 0 && cfg.occupancy != 6 && cfg.occupancy != 8 && cfg.occupancy != 10)
+        throw Error(WFB_ERR_INVALID_ARGUMENT, "wavefront occupancy target must be 0, 6, 8 or 10");
+    state_->kernel = wavefront_kernel<false>(cfg.occupancy);
+    state_->kernel_multi = wavefront_kernel<true>(cfg.occupancy);
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, state_->kernel, kWfBlock, 0), "occupancy");
     if (occ < 1) throw Error(WFB_ERR_UNSUPPORTED, "wavefront kernel does not fit on an SM");
     state_->grid = sms * occ;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wavefront_persistent<true>, kWfBlock, 0), "occupancy");
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, state_->kernel_multi, kWfBlock, 0), "occupancy");
     if (occ < 1) throw Error(WFB_ERR_UNSUPPORTED, "wavefront batch kernel does not fit on an SM");
     state_->grid_multi = sms * occ;
 }
@@ -684,8 +757,7 @@ void WavefrontEngine::reserve_direct() {
 namespace {
 
 // Control reset, pool init, the cooperative launch and the counter fold; returns kernels launched.
-template <bool MULTI>
-int launch_pool(const WfArgs& args, int grid, int capacity, DevCounters* counters, bool count_rays,
+int launch_pool(WfKernel kernel, const WfArgs& args, int grid, int capacity, DevCounters* counters, bool count_rays,
                 size_t window_bytes, float hit_ratio, cudaStream_t stream, KernelTimer* timer = nullptr) {
     const Pool& pool = args.pool;
     cuda_check(cudaMemsetAsync(pool.ctl, 0, sizeof(Control), stream), "memset control");
@@ -719,7 +791,7 @@ int launch_pool(const WfArgs& args, int grid, int capacity, DevCounters* counter
     lc.attrs = attr;
     lc.numAttrs = n_attr;
     if (timer) timer->begin(stream);
-    cuda_check(cudaLaunchKernelEx(&lc, wavefront_persistent<MULTI>, a), "wavefront cooperative launch");
+    cuda_check(cudaLaunchKernelEx(&lc, kernel, a), "wavefront cooperative launch");
     if (timer) timer->end(stream);
     wavefront_fold<<<1, 1, 0, stream>>>(pool.ctl, counters, count_rays ? 1 : 0);
     cuda_check(cudaGetLastError(), "wavefront fold launch");
@@ -770,7 +842,8 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
     a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = p.stage_timing ? 1 : 0;
-    int launches = launch_pool<false>(a, st.grid, capacity_, counters, p.count_rays, st.window_bytes, st.hit_ratio,
+    a.suspend = cfg_.suspend_stragglers ? 1 : 0;
+    int launches = launch_pool(st.kernel, a, st.grid, capacity_, counters, p.count_rays, st.window_bytes, st.hit_ratio,
                                       stream, timer);
     if (a.job0.chunks > 1) {
         launch_film_commit(film, a.job0.lbuf, p.sample_count, stream);
@@ -804,7 +877,8 @@ int WavefrontEngine::run_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, 
     a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = 0;
-    return launch_pool<true>(a, state_->grid_multi, capacity_, counters, count_rays, state_->window_bytes,
+    a.suspend = cfg_.suspend_stragglers ? 1 : 0;
+    return launch_pool(state_->kernel_multi, a, state_->grid_multi, capacity_, counters, count_rays, state_->window_bytes,
                              state_->hit_ratio, stream);
 }
 

@@ -176,7 +176,7 @@ uint64_t wfb_renderer_device_bytes(wfb_renderer_t r);
  * pixel (0: automatic), occupancy target (block 128: 0 none, 6, 8 or 10 CTAs per SM by a register
  * cap), and leaf_batch (1..32): a warp runs a round of primitive tests once this many of its
  * lanes hold a pending leaf (or they outnumber the lanes testing boxes). Wavefront: paths in
- * flight, min_active and leaf_batch. */
+ * flight, min_active, leaf_batch and occupancy (0, 6, 8 or 10 CTAs of 128 threads per SM). */
 int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int min_active,
                            int split_chunks, int paths_in_flight, int occupancy, int leaf_batch);
 /* Wavefront path pool resident in L2 (no reference counterpart; the reference's pool is W*H paths
@@ -203,6 +203,7 @@ typedef struct {
     int paths_in_flight, wf_min_active;
     double msamples_s, megakernel_msamples_s, wavefront_msamples_s;
     int candidates;
+    int wf_occupancy; /* wavefront register cap: 0, 6, 8 or 10 CTAs of 128 threads per SM */
 } wfb_tune_result;
 int wfb_autotune(wfb_scene_t scene, int width, int height, int probe_spp, int max_depth, int try_wavefront,
                  wfb_tune_result* out);
@@ -218,10 +219,11 @@ typedef struct {
     int mode;            /* WFB_MODE_MEGAKERNEL or WFB_MODE_WAVEFRONT */
     int use_graph;       /* megakernel: replay one captured CUDA graph per launch shape */
     int block;           /* megakernel: 64, 128 or 256 threads; <= 0: 128 */
-    int occupancy;       /* megakernel, block 128: 0, 6, 8 or 10 CTAs per SM by a register cap; < 0: 8 */
+    int occupancy;       /* register cap for 0, 6, 8 or 10 CTAs per SM: megakernel (block 128; < 0: 8)
+                            and wavefront (128-thread blocks; < 0: 10) */
     int min_active;      /* 1..32; <= 0: default */
     int leaf_batch;      /* 1..32; <= 0: default (see wfb_renderer_configure) */
-    int paths_in_flight; /* wavefront pool slots; <= 0: 4M */
+    int paths_in_flight; /* wavefront pool slots; <= 0: 8M */
     int split_chunks;    /* megakernel: work units per pixel of each job; <= 0: automatic (one
                             sample per unit while the job's per-sample buffer fits) */
 } wfb_launch_config;
