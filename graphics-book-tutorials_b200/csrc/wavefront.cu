@@ -682,13 +682,16 @@ size_t reserve_persisting_l2(size_t want, int dev) {
 
 }  // namespace
 
-size_t wavefront_slot_bytes() { return pool_bytes(1 << 20, nullptr, nullptr) >> 20; }
+size_t wavefront_slot_bytes() { return (pool_bytes(1 << 20, nullptr, nullptr) + (1 << 20) - 1) >> 20; }
 
 size_t wavefront_l2_resident_paths(int device) {
     int max_persist = 0;
     cuda_check(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, device), "persisting L2 size");
-    const size_t slots = (size_t)std::max(max_persist, 0) / wavefront_slot_bytes();
-    return slots & ~(size_t)(kWfBlock - 1);
+    if (max_persist <= 0) return 0;
+    // the largest multiple of the block whose whole arena fits the set-aside
+    size_t slots = ((size_t)max_persist / wavefront_slot_bytes()) & ~(size_t)(kWfBlock - 1);
+    while (slots > 0 && pool_bytes((int)slots, nullptr, nullptr) > (size_t)max_persist) slots -= kWfBlock;
+    return slots;
 }
 
 WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixels_(pixels), cfg_(cfg) {
