@@ -19,12 +19,12 @@ constexpr int kScheduleExpress = 0;
 constexpr int kScheduleShared = 1;
 
 struct SliceJob {
-    double pixels;  // width * height
+    double cost;    // predicted cost of one sample of every pixel of the job (e.g. ms)
     int remaining;  // samples per pixel not yet issued (> 0)
 };
 
 // Samples per pixel of each job (in admission order) for the next launch; 0 leaves a job out.
-// `budget` is the launch's sample budget (pixels x samples). At least one job advances.
+// `budget` is the launch's cost budget, in the unit of SliceJob::cost. At least one job advances.
 inline std::vector<int> plan_slices(const std::vector<SliceJob>& jobs, double budget, int schedule) {
     std::vector<int> k(jobs.size(), 0);
     if (jobs.empty()) return k;
@@ -32,7 +32,7 @@ inline std::vector<int> plan_slices(const std::vector<SliceJob>& jobs, double bu
         // the largest common slice whose total stays within the budget (at least one sample)
         auto total = [&](int s) {
             double t = 0.0;
-            for (const SliceJob& j : jobs) t += j.pixels * std::min(s, j.remaining);
+            for (const SliceJob& j : jobs) t += j.cost * std::min(s, j.remaining);
             return t;
         };
         int lo = 1, hi = 1;
@@ -50,7 +50,7 @@ inline std::vector<int> plan_slices(const std::vector<SliceJob>& jobs, double bu
     double left = budget;
     bool any = false;
     for (size_t i = 0; i < jobs.size(); ++i) {
-        const double work = jobs[i].pixels * jobs[i].remaining;
+        const double work = jobs[i].cost * jobs[i].remaining;
         if (work <= small && (work <= left || !any)) {
             k[i] = jobs[i].remaining;
             left -= work;
@@ -59,13 +59,13 @@ inline std::vector<int> plan_slices(const std::vector<SliceJob>& jobs, double bu
     }
     bool oldest_large = true;
     for (size_t i = 0; i < jobs.size(); ++i) {
-        if (k[i] > 0 || jobs[i].pixels * jobs[i].remaining <= small) continue;
+        if (k[i] > 0 || jobs[i].cost * jobs[i].remaining <= small) continue;
         const double share = oldest_large ? std::max(left, small) : left;
-        int s = (int)std::min<double>(jobs[i].remaining, std::floor(share / jobs[i].pixels));
+        int s = (int)std::min<double>(jobs[i].remaining, std::floor(share / jobs[i].cost));
         if (s < 1 && (oldest_large || !any)) s = 1;  // the oldest large job always advances
         if (s < 1) break;                             // later large jobs wait their turn
         k[i] = s;
-        left -= jobs[i].pixels * s;
+        left -= jobs[i].cost * s;
         any = true;
         oldest_large = false;
     }

@@ -34,6 +34,7 @@ double now_seconds() {
 
 struct Server::Job {
     JobSpec spec;
+    uint64_t rate_key = 0;  // class of its rendering rate (scene content, depth limit)
     int state = kQueued;
     int done = 0;      // samples added to the film so far (launches finished)
     int issued = 0;    // samples enqueued (launches finished or in flight)
@@ -114,6 +115,7 @@ uint64_t Server::submit(const JobSpec& job) {
     if (job.sample_count <= 0 || job.max_depth < 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "bad spp or depth");
     auto j = std::make_unique<Job>();
     j->spec = job;
+    j->rate_key = mix_key(job.scene->content_key, &job.max_depth, sizeof(job.max_depth));
     j->spec.first_sample = 0;
     j->t_arrival = now_seconds();
     uint64_t ticket;
@@ -243,7 +245,13 @@ bool Server::admit_locked() {
     return any;
 }
 
-// Samples of each admitted job (in admission order) for the next launch; 0 leaves a job out.
+double Server::class_rate(uint64_t key) const {
+    auto it = class_msps_.find(key);
+    return it != class_msps_.end() ? it->second : msps_default_;
+}
+
+// Samples of each admitted job (in admission order) for the next launch; 0 leaves a job out. The
+// budget is the launch's target length; a job's cost per sample is its pixels at its class's rate.
 std::vector<int> Server::plan_launch(const std::vector<Job*>& act) {
     std::vector<int> k(act.size(), 0);
     for (size_t i = 0; i < act.size(); ++i) {
@@ -253,9 +261,11 @@ std::vector<int> Server::plan_launch(const std::vector<Job*>& act) {
     }
     if (cfg_.one_job_per_launch || cfg_.fixed_slice > 0) return k;
     std::vector<SliceJob> jobs(act.size());
-    for (size_t i = 0; i < act.size(); ++i)
-        jobs[i] = SliceJob{(double)act[i]->spec.width * act[i]->spec.height, act[i]->spec.sample_count - act[i]->issued};
-    return plan_slices(jobs, msps_estimate_ * 1e3 * cfg_.launch_target_ms, cfg_.schedule);
+    for (size_t i = 0; i < act.size(); ++i) {
+        const double pixels = (double)act[i]->spec.width * act[i]->spec.height;
+        jobs[i] = SliceJob{pixels / (class_rate(act[i]->rate_key) * 1e3), act[i]->spec.sample_count - act[i]->issued};
+    }
+    return plan_slices(jobs, cfg_.launch_target_ms, cfg_.schedule);
 }
 
 // Two launches in flight: while the GPU renders launch N, the worker retires launch N-1's
@@ -268,6 +278,7 @@ void Server::worker() {
         std::vector<Job*> jobs;
         std::vector<uint64_t> tickets;
         std::vector<int> counts;  // samples of each job in this launch
+        std::vector<double> pred_ms;  // predicted device time of each job's slice
         uint64_t samples = 0;
         int slot = 0;
         std::string err;
@@ -318,6 +329,7 @@ void Server::worker() {
                 sp.sample_count = plan[i];
                 f.samples += (uint64_t)sp.width * sp.height * sp.sample_count;
                 f.counts.push_back(sp.sample_count);
+                f.pred_ms.push_back((double)sp.width * sp.height * sp.sample_count / (class_rate(j->rate_key) * 1e3));
                 JobBuffers b = j->buf;
                 b.chunks = std::min(b.chunks, sp.sample_count);
                 if (b.chunks > 1 && b.lbuf == nullptr) b.chunks = 1;
@@ -360,10 +372,18 @@ void Server::worker() {
         // Only launches that filled most of their budget refine the rate: a launch carrying a few
         // small jobs is dominated by its ramp-up and tail, and its low rate would shrink every
         // following slice (large jobs would then crawl through many short launches).
-        const double budget = msps_estimate_ * 1e3 * cfg_.launch_target_ms;
-        if (done.err.empty() && ms > 0.f && (double)done.samples >= 0.5 * budget) {
-            const double rate = (double)done.samples / (ms * 1e3);  // Msamples/s
-            msps_estimate_ = 0.7 * msps_estimate_ + 0.3 * rate;
+        // Refine the rates: each class in the launch moves by the ratio of predicted to measured
+        // time, weighted by its share of the prediction (a launch holding one class corrects it
+        // fully over a few launches; minor members barely move).
+        double pred = 0.0;
+        for (double v : done.pred_ms) pred += v;
+        if (done.err.empty() && ms > 0.f && pred >= 0.5 * cfg_.launch_target_ms) {
+            const double ratio = std::clamp(pred / (double)ms, 0.25, 4.0);
+            std::map<uint64_t, double> share;
+            for (size_t i = 0; i < done.jobs.size(); ++i) share[done.jobs[i]->rate_key] += done.pred_ms[i] / pred;
+            for (const auto& [key, w] : share) class_msps_[key] = class_rate(key) * std::pow(ratio, 0.5 * w);
+            const double rate = (double)done.samples / ((double)ms * 1e3);  // Msamples/s over every class
+            msps_default_ = 0.7 * msps_default_ + 0.3 * rate;
         }
         // Jobs this launch finished go to the download thread: no later launch touches their films,
         // so the copies overlap the launch in flight and the worker goes on enqueueing.

@@ -20,7 +20,7 @@ static int g_cases = 0;
 
 static double work(const std::vector<SliceJob>& j, const std::vector<int>& k) {
     double s = 0;
-    for (size_t i = 0; i < j.size(); ++i) s += j[i].pixels * k[i];
+    for (size_t i = 0; i < j.size(); ++i) s += j[i].cost * k[i];
     return s;
 }
 
@@ -95,8 +95,8 @@ int main() {
             // oldest large job; shared: every job advances at least one sample
             double biggest = 0, all = 0;
             for (const auto& x : j) {
-                biggest = std::max(biggest, x.pixels);
-                all += x.pixels;
+                biggest = std::max(biggest, x.cost);
+                all += x.cost;
             }
             if (s == wfb::kScheduleExpress) CHECK(work(j, k) <= 1.25 * b + biggest + 1);
             else CHECK(work(j, k) <= std::max(b, all) + 1);
