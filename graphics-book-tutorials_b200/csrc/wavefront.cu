@@ -49,8 +49,8 @@ struct Control {
     unsigned fetch[2];   // extend, shadow dynamic-fetch cursors
     unsigned unit_next;
     unsigned ticket;
-    unsigned retired[2];  // items finished in the current extend / shadow phase
-    unsigned suspended;   // rays parked for the next iteration (all phases)
+    unsigned retired;    // extension rays finished in the current E phase
+    unsigned suspended;  // extension rays carried over to the next iteration (all phases)
     unsigned err;
     unsigned overflow;
     unsigned invalid;
@@ -69,13 +69,13 @@ struct Pool {
     int4* unit;      // pixel (-1: none), sample, end sample, 0
     float4* acc;     // film sums of the unit (direct mode only; outside the pool arena): rgb, lum
     float* acc2;     // lum2
-    float4* hit;     // t, prim, u, v (a parked extension ray: its best hit so far)
-    int2* trav;      // a parked ray's traversal state: next node, pending leaf
-    uint32_t* alive;  // slot state: kNoPath, kLive, kExtParked, kShadowLive, kShadowLast
+    float4* hit;     // t, prim, u, v (a suspended ray: its best hit so far)
+    int2* trav;      // a suspended ray's traversal state: next node, pending leaf
+    uint32_t* alive;  // 0: no path, 1: path with a ray to trace, 2: extension ray suspended mid-traversal
     uint32_t* list[2];
     uint32_t* queue[4];  // lambert, metal, dielectric, shadow slots
-    float4* sh_dir;      // shadow record of a slot: direction, tmax
-    float4* sh_c;        // contribution
+    float4* sh_dir;      // shadow records: direction, tmax
+    float4* sh_c;        // contribution, owner slot
     unsigned long long* status;
     Control* ctl;
 };
@@ -172,40 +172,27 @@ __device__ bool grid_sync(Control* c, unsigned nblocks, int stage, unsigned long
     return s_ok != 0;
 }
 
-// Slot states (Pool::alive).
-constexpr uint32_t kNoPath = 0;       // no path (ended: committed and regenerated by the next R phase)
-constexpr uint32_t kLive = 1;         // a path with a ray to trace
-constexpr uint32_t kExtParked = 2;    // extension ray suspended mid-traversal (state in trav, hit)
-constexpr uint32_t kShadowLive = 3;   // shadow ray suspended; the path goes on after it
-constexpr uint32_t kShadowLast = 4;   // shadow ray suspended; the path ends after it
-
-// Resumable closest-hit / any-hit traversal over a list of slots fetched dynamically: the active
-// list (extend) or the shadow queue (shadow; a slot's shadow record is sh_dir/sh_c[slot]).
+// Resumable closest-hit / any-hit traversal over a list of rays fetched dynamically.
+// Extend: items[i] are slot ids. Shadow: the rays are shadow records 0..n-1 (items unused).
 //
-// Stragglers: a phase ends when its last ray does, and near the end a few long rays keep whole
-// warps (and the grid barrier) waiting. Once `suspend_at` of the phase's n items are done, a warp
-// with nothing left to fetch parks its unfinished rays instead -- next node and pending leaf in
-// trav, an extension ray's best hit in hit -- and leaves. A parked extension ray (kExtParked)
-// resumes from exactly that state in the next extend phase, its slot skipping this bounce's
-// classify and shading. A parked shadow ray (kShadowLive / kShadowLast) is finished by its slot's
-// next extend item before anything else: the unoccluded contribution lands in L before the next
-// classify, as in trace_path (WVM/include/wf/path_core.hpp:279-304), and then the extension ray is
-// traced (kShadowLive) or the path ends (kShadowLast). The traversal steps are the same either way,
-// so hits and films are the same bits.
+// Extension stragglers: the phase ends when its last ray does, and near the end a few long rays
+// keep whole warps (and the grid barrier) waiting. Once `suspend_at` of the phase's n rays have
+// finished, a warp that has nothing left to fetch parks its unfinished rays instead -- next node,
+// pending leaf and best hit into the pool, slot state 2 -- and leaves; the slot skips this bounce's
+// classify and shading, stays in the active list, and its ray resumes from exactly that state in
+// the next iteration's extend phase. The traversal steps are the same, so the hit is the same.
 template <bool SHADOW, bool MULTI>
 __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned n, unsigned* cursor,
-                               unsigned long long* n_ext, unsigned long long* n_sh, unsigned* retired,
-                               unsigned suspend_at) {
+                               unsigned long long* n_rays, unsigned* retired = nullptr,
+                               unsigned suspend_at = 0xffffffffu) {
     const Pool& P = a.pool;
     // BVH of the lane's current ray: a batch reads its job's from the table at fetch time
     const float4* nodes = a.job0.s.nodes;
     const float4* prims = a.job0.s.prims;
     int n_nodes = a.job0.s.n_nodes, n_spheres = a.job0.s.n_spheres;
     const int lane = threadIdx.x & 31;
-    int item = -1;     // list position, -1: none
-    int slot = 0;      // slot of the current item
-    bool anyhit = SHADOW;
-    uint32_t after = kNoPath;  // extend items finishing a parked shadow ray: the state it leaves
+    int item = -1;  // list position, -1: none
+    uint32_t id = 0;  // slot (extend) or shadow record (shadow) of the current ray
     int node = -1;
     int pend = 0;  // pending leaf (box_step / prim_step)
     wf::Vec3 o{0.f, 0.f, 0.f};
@@ -228,7 +215,9 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
                 const unsigned i = base + __popc(nm & ((1u << lane) - 1u));
                 if (i < n) {
                     item = (int)i;
-                    slot = (int)items[i];
+                    id = SHADOW ? i : items[i];  // shadow records are numbered by queue position
+                    // every ray starts at its path's origin with tmin = kRayEps (see TravRay)
+                    const int slot = SHADOW ? __float_as_int(P.sh_c[id].w) : (int)id;
                     if (MULTI) {
                         const DevScene& js = a.jobs[P.unit[slot].w].s;
                         nodes = js.nodes;
@@ -236,29 +225,21 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
                         n_nodes = js.n_nodes;
                         n_spheres = js.n_spheres;
                     }
-                    // every ray starts at its path's origin with tmin = kRayEps (see TravRay); the
-                    // shadow ray of a Lambertian bounce starts where the next extension ray does
                     const float4 oo = P.ray_o[slot];
+                    const float4 d = SHADOW ? P.sh_dir[id] : P.ray_d[id];
                     o = wf::Vec3{oo.x, oo.y, oo.z};
-                    const uint32_t st = SHADOW ? kLive : P.alive[slot];
-                    anyhit = SHADOW || st == kShadowLive || st == kShadowLast;
-                    const float4 d = anyhit ? P.sh_dir[slot] : P.ray_d[slot];
                     traversal_begin(n_nodes, wf::Vec3{d.x, d.y, d.z}, d.w, &ray, &node, &h);
                     pend = 0;
-                    if (!SHADOW && (st == kExtParked || anyhit)) {  // resume a parked ray where it stopped
+                    if (!SHADOW && P.alive[slot] == 2u) {  // resume a suspended ray where it stopped
                         const int2 tv = P.trav[slot];
+                        const float4 hv = P.hit[slot];
                         node = tv.x;
                         pend = tv.y;
-                        if (st == kExtParked) {
-                            const float4 hv = P.hit[slot];
-                            h.t = hv.x;
-                            h.prim = __float_as_int(hv.y);
-                            h.u = hv.z;
-                            h.v = hv.w;
-                            P.alive[slot] = kLive;
-                        } else {
-                            after = st == kShadowLive ? kLive : kNoPath;
-                        }
+                        h.t = hv.x;
+                        h.prim = __float_as_int(hv.y);
+                        h.u = hv.z;
+                        h.v = hv.w;
+                        P.alive[slot] = 1u;
                     }
                 } else {
                     exhausted = true;
@@ -277,67 +258,57 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
             const unsigned tm = pm | bm;
             if (tm == 0) break;
             if (__popc(tm) < a.min_active && __ballot_sync(kFull, !(in_leaf || at_box) && !exhausted) != 0) break;
-            if ((++round & 31u) == 0u && __ballot_sync(kFull, exhausted) != 0) {
-                // nothing left to fetch: park the warp's rays once most of the phase is done
+            if (!SHADOW && (++round & 31u) == 0u && __ballot_sync(kFull, exhausted) != 0) {
+                // nothing left to fetch: suspend the warp's rays once most of the phase is done
                 unsigned done = 0;
                 if (lane == 0) done = *(volatile unsigned*)retired;
                 done = __shfl_sync(kFull, done, 0);
                 if (done >= suspend_at) {
+                    // every lane holding an item parks it, finished ones included: the saved best
+                    // hit makes a finished ray retire with its result on resumption
                     const unsigned sm = __ballot_sync(kFull, item >= 0);
                     if (item >= 0) {
-                        P.trav[slot] = make_int2(node, pend);
-                        if (!anyhit) {
-                            P.hit[slot] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
-                            P.alive[slot] = kExtParked;
-                        } else if (SHADOW) {  // shading left the path live (1) or ended (0)
-                            P.alive[slot] = P.alive[slot] != kNoPath ? kShadowLive : kShadowLast;
-                        }  // else: a resumed shadow ray, parked again in the same state
+                        P.trav[id] = make_int2(node, pend);
+                        P.hit[id] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
+                        P.alive[id] = 2u;
                         item = -1;
                         node = -1;
                         pend = 0;
                     }
-                    if (lane == 0) atomicAdd(&P.ctl->suspended, (unsigned)__popc(sm));
+                    if (lane == 0) atomicAdd(&a.pool.ctl->suspended, (unsigned)__popc(sm));
                     return;
                 }
             }
             const int np = __popc(pm);
             if (np != 0 && (np >= a.leaf_batch || np >= __popc(bm))) {
-                if (in_leaf) prim_step(prims, n_spheres, o, ray, anyhit, node, pend, h);
+                if (in_leaf) prim_step(prims, n_spheres, o, ray, SHADOW, node, pend, h);
             } else if (at_box) {
                 box_step(nodes, n_nodes, o, ray, h.t, node, pend);
             }
         }
         // retire finished rays
-        bool fin = item >= 0 && node < 0 && pend == 0;
+        const bool fin = item >= 0 && node < 0 && pend == 0;
+        if (!SHADOW) {
+            const unsigned fm = __ballot_sync(kFull, fin);
+            if (fm && lane == __ffs(fm) - 1) atomicAdd(retired, (unsigned)__popc(fm));
+        }
         if (fin) {
-            if (anyhit) {
-                ++*n_sh;
+            ++*n_rays;
+            if (SHADOW) {
                 if (h.prim < 0) {  // unoccluded: L += contrib
-                    const float4 c = P.sh_c[slot];
+                    const float4 c = P.sh_c[id];
+                    const int slot = __float_as_int(c.w);
                     float4 l = P.rad[slot];
                     l.x += c.x;
                     l.y += c.y;
                     l.z += c.z;
                     P.rad[slot] = l;
                 }
-                if (!SHADOW) {
-                    P.alive[slot] = after;
-                    if (after == kLive) {  // now the slot's extension ray, on the same lane
-                        const float4 d = P.ray_d[slot];
-                        traversal_begin(n_nodes, wf::Vec3{d.x, d.y, d.z}, d.w, &ray, &node, &h);
-                        pend = 0;
-                        anyhit = false;
-                        fin = false;
-                    }
-                }
             } else {
-                ++*n_ext;
-                P.hit[slot] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
+                P.hit[id] = make_float4(h.t, __int_as_float(h.prim), h.u, h.v);
             }
+            item = -1;
         }
-        const unsigned fm = __ballot_sync(kFull, fin);
-        if (fm && lane == __ffs(fm) - 1) atomicAdd(retired, (unsigned)__popc(fm));
-        if (fin) item = -1;
     }
 }
 
@@ -372,7 +343,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
         if (gtid == 0) {
             c->qcount[0] = c->qcount[1] = c->qcount[2] = c->qcount[3] = 0;
             c->fetch[0] = c->fetch[1] = 0;
-            c->retired[0] = c->retired[1] = 0;
+            c->retired = 0;
         }
         const unsigned ntiles = (n_act + kWfBlock - 1) / kWfBlock;
         for (;;) {
@@ -386,7 +357,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
             bool has_path = false, need_unit = false;
             int4 u = make_int4(-1, 0, 0, 0);
             if (valid) {
-                has_path = P.alive[slot] != kNoPath;
+                has_path = P.alive[slot] != 0u;
                 if (!has_path) {
                     u = P.unit[slot];
                     if (u.x >= 0) {
@@ -416,7 +387,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
                             const int px = u.x % J.s.width, py = u.x / J.s.width;
                             store_path(P, slot, wf::init_path(J.s, px, py, (uint32_t)u.y, J.seed));
                             P.unit[slot] = u;
-                            P.alive[slot] = kLive;
+                            P.alive[slot] = 1u;
                             has_path = true;
                         } else {
                             if (!split) {
@@ -461,7 +432,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
                             P.acc2[slot] = J.film.lum2[pixel];
                         }
                         store_path(P, slot, wf::init_path(J.s, pixel % J.s.width, pixel / J.s.width, (uint32_t)first, J.seed));
-                        P.alive[slot] = kLive;
+                        P.alive[slot] = 1u;
                         has_path = true;
                     }
                 }
@@ -496,8 +467,8 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
         if (n == 0) break;
 
         // ---------------- E: extension rays ----------------
-        // stragglers may be parked once 95% of a large phase's items are done
-        traverse_phase<false, MULTI>(a, next, n, &c->fetch[0], &n_ext, &n_sh, &c->retired[0],
+        // stragglers may be suspended once 95% of a large phase's rays have finished
+        traverse_phase<false, MULTI>(a, next, n, &c->fetch[0], &n_ext, &c->retired,
                                      a.suspend && n >= 4096 ? n - n / 20 : 0xffffffffu);
         if (!grid_sync(c, nblocks, 0, &t_last, a.wait_ns)) break;
 
@@ -507,7 +478,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
             const bool valid = i < n;
             const int slot = valid ? (int)next[i] : 0;
             int mat = -1;
-            if (valid && P.alive[slot] == kLive) {  // parked rays have no hit yet; ended paths none
+            if (valid && P.alive[slot] != 2u) {  // a suspended ray has no hit yet
                 const float4 hv = P.hit[slot];
                 wf::HitRecord h;
                 h.t = hv.x;
@@ -523,12 +494,12 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
                 wf::Surface f;
                 mat = wf::classify(J.s, ps, h, J.max_depth, &f);
                 store_radiance(P, slot, ps);
-                if (mat < 0) P.alive[slot] = kNoPath;
+                if (mat < 0) P.alive[slot] = 0u;
             }
             for (int q = 0; q < 3; ++q) {
                 const bool mine = valid && mat == q;
                 const uint32_t at = queue_push(P.queue[q], &c->qcount[q], a.qcap, (uint32_t)slot, mine, &c->overflow);
-                if (mine && at == 0xFFFFFFFFu) P.alive[slot] = kNoPath;  // dropped on overflow: the path ends
+                if (mine && at == 0xFFFFFFFFu) P.alive[slot] = 0u;  // dropped on overflow: the path ends
             }
         }
         if (!grid_sync(c, nblocks, 1, &t_last, a.wait_ns)) break;
@@ -571,14 +542,14 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
                         alive = wf::shade_dielectric(s, ps, f);
                     }
                     store_path(P, slot, ps);
-                    P.alive[slot] = alive ? kLive : kNoPath;
+                    P.alive[slot] = alive ? 1u : 0u;
                 }
                 if (q == wf::kLambert) {
-                    if (push) {
-                        P.sh_dir[slot] = make_float4(sh.d.x, sh.d.y, sh.d.z, sh.tmax);
-                        P.sh_c[slot] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                    const uint32_t at = queue_push(P.queue[3], &c->qcount[3], a.qcap, (uint32_t)slot, push, &c->overflow);
+                    if (push && at != 0xFFFFFFFFu) {
+                        P.sh_dir[at] = make_float4(sh.d.x, sh.d.y, sh.d.z, sh.tmax);
+                        P.sh_c[at] = make_float4(contrib.x, contrib.y, contrib.z, __int_as_float(slot));
                     }
-                    queue_push(P.queue[3], &c->qcount[3], a.qcap, (uint32_t)slot, push, &c->overflow);
                 }
             }
             if (a.split_shading && !grid_sync(c, nblocks, 2 + q, &t_last, a.wait_ns)) ok = false;
@@ -589,8 +560,7 @@ __global__ void __launch_bounds__(kWfBlock, MINB) wavefront_persistent(const WfA
         // ---------------- H: shadow rays ----------------
         const unsigned nsh = min(*(volatile unsigned*)&c->qcount[3], a.qcap);
         if (gtid == 0 && nsh > c->high_water[3]) c->high_water[3] = nsh;
-        traverse_phase<true, MULTI>(a, P.queue[3], nsh, &c->fetch[1], &n_ext, &n_sh, &c->retired[1],
-                                    a.suspend && nsh >= 4096 ? nsh - nsh / 20 : 0xffffffffu);
+        traverse_phase<true, MULTI>(a, nullptr, nsh, &c->fetch[1], &n_sh);
         if (!grid_sync(c, nblocks, 5, &t_last, a.wait_ns)) break;
     }
 
@@ -628,7 +598,7 @@ __global__ void wavefront_init(Pool P, int capacity) {
     }
     if (i < capacity) {
         P.list[0][i] = (uint32_t)i;
-        P.alive[i] = kNoPath;
+        P.alive[i] = 0u;
         P.unit[i] = make_int4(-1, 0, 0, 0);
     }
 }
