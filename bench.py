@@ -352,6 +352,8 @@ def main():
     ap.add_argument("--lambdas", default="5,10,20,50,100,200")
     ap.add_argument("--duration", type=float, default=60.0)
     ap.add_argument("--schedules", default="express", help="serve mode: continuous-batching schedules to run")
+    ap.add_argument("--launch-target-ms", type=float, default=20.0, help="serve mode: length the server aims each launch at")
+    ap.add_argument("--no-plain", action="store_true", help="serve mode: skip the one-job-per-launch baseline")
     ap.add_argument("--no-batch-serve", action="store_true", help="skip the batched/served summary in render mode")
     args = ap.parse_args()
     if args.gpus < 1:
@@ -396,8 +398,11 @@ def main():
             print(json.dumps(out), flush=True)
         else:
             for lam in [float(x) for x in args.lambdas.split(",")]:
-                for plain, schedule in [(False, s) for s in args.schedules.split(",")] + [(True, "express")]:
-                    r = bench_serve(wfb, scenes, lam, args.duration, plain=plain, schedule=schedule)
+                runs = [(False, s) for s in args.schedules.split(",") if s] + ([] if args.no_plain else [(True, "express")])
+                for plain, schedule in runs:
+                    r = bench_serve(wfb, scenes, lam, args.duration, plain=plain, schedule=schedule,
+                                    target_ms=args.launch_target_ms)
+                    r["launch_target_ms"] = args.launch_target_ms
                     print(json.dumps({"mode": "serve", **r}), flush=True)
         group.close()
         return
