@@ -98,10 +98,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def read_profile():
-    """`key: number` lines of the committed ncu summary of the megakernel (issue activity, lanes per
-    instruction, DRAM bytes of a full-size launch), or {} if absent."""
-    path = os.path.join(PROFILE_DIR, "megakernel_icospheres.txt")
+def read_profile(kernel="megakernel", scene="icospheres"):
+    """`key: number` lines of the committed ncu summary of a kernel on a scene (issue activity, lanes
+    per instruction, DRAM bytes of a full-size launch), or {} if absent."""
+    path = os.path.join(PROFILE_DIR, f"{kernel}_{scene}.txt")
     out = {}
     if not os.path.exists(path):
         return out
@@ -353,6 +353,10 @@ def main():
     ap.add_argument("--duration", type=float, default=60.0)
     ap.add_argument("--schedules", default="express", help="serve mode: continuous-batching schedules to run")
     ap.add_argument("--launch-target-ms", type=float, default=20.0, help="serve mode: length the server aims each launch at")
+    ap.add_argument("--paths-in-flight", type=int, default=0, help="wavefront pool slots with --no-tune (profiling cases)")
+    ap.add_argument("--wf-occupancy", type=int, default=-1, help="wavefront register cap (0, 6, 8, 10) with --no-tune")
+    ap.add_argument("--l2-residency", type=int, default=None, choices=[-1, 0, 1],
+                    help="wavefront pool under a persisting L2 window: -1 when it fits, 0 never, 1 always")
     ap.add_argument("--no-plain", action="store_true", help="serve mode: skip the one-job-per-launch baseline")
     ap.add_argument("--no-batch-serve", action="store_true", help="skip the batched/served summary in render mode")
     args = ap.parse_args()
@@ -421,6 +425,11 @@ def main():
     renderer = wfb.GpuRenderer(scene, mode)
     if tuning is not None:
         renderer.apply_tuning(tuning)
+    if mode == wfb.WAVEFRONT and (args.paths_in_flight > 0 or args.wf_occupancy >= 0):
+        renderer.configure(paths_in_flight=args.paths_in_flight if args.paths_in_flight > 0 else -1,
+                           occupancy=args.wf_occupancy)
+    if mode == wfb.WAVEFRONT and args.l2_residency is not None:
+        renderer.set_l2_residency(args.l2_residency)
     params = wfb.RenderParams(spp=SPP, seed=SEED, max_depth=DEPTH)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
@@ -484,7 +493,7 @@ def main():
     bytes_per_sample = 224.0 * ext_ps + 96.0 * sh_ps + 40.0
     kernel_ms = group.max(float(sum(kern_ms))) / args.steps  # mean launch duration of the dominant kernel
     achieved = samples * bytes_per_sample / (kernel_ms / 1e3) / 1e9
-    prof = read_profile()
+    prof = read_profile("megakernel" if mode == wfb.MEGAKERNEL else "wavefront", SCENE)
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
@@ -517,6 +526,15 @@ def main():
         "clocks": clk,
         "device": wfb.device_name(),
     }
+    if mode == wfb.WAVEFRONT:
+        # untimed: one render with the stage clock (%globaltimer at the grid barriers; the shading
+        # queues get a barrier each), and the pool's shape
+        sst = wfb.RenderStats()
+        renderer.render(wfb.RenderParams(spp=SPP, seed=SEED, max_depth=DEPTH, stage_timing=True), sst)
+        line["wavefront"] = {"stages_ms": {k: round(v, 2) for k, v in sst.stages.items()},
+                             "staged_render_ms": round(sst.render_ms, 2),
+                             "l2_window_bytes": renderer.l2_window_bytes(), "device_bytes": renderer.device_bytes(),
+                             "paths_in_flight": args.paths_in_flight or (tuning.paths_in_flight if tuning else None)}
     if rank == 0 and not args.no_batch_serve:
         scenes = mix_scenes(wfb)
         line["batched"] = bench_batch(wfb, scenes, repeats=1)

@@ -279,11 +279,16 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
                     return;
                 }
             }
+            // a single-job launch reads its BVH from parameter space, keeping registers for the ray
             const int np = __popc(pm);
             if (np != 0 && (np >= a.leaf_batch || np >= __popc(bm))) {
-                if (in_leaf) prim_step(prims, n_spheres, o, ray, SHADOW, node, pend, h);
+                if (in_leaf) {
+                    if (MULTI) prim_step(prims, n_spheres, o, ray, SHADOW, node, pend, h);
+                    else prim_step(a.job0.s.prims, a.job0.s.n_spheres, o, ray, SHADOW, node, pend, h);
+                }
             } else if (at_box) {
-                box_step(nodes, n_nodes, o, ray, h.t, node, pend);
+                if (MULTI) box_step(nodes, n_nodes, o, ray, h.t, node, pend);
+                else box_step(a.job0.s.nodes, a.job0.s.n_nodes, o, ray, h.t, node, pend);
             }
         }
         // retire finished rays
