@@ -247,7 +247,12 @@ bool Server::admit_locked() {
 
 double Server::class_rate(uint64_t key) const {
     auto it = class_msps_.find(key);
-    return it != class_msps_.end() ? it->second : msps_default_;
+    if (it != class_msps_.end()) return it->second;
+    // an unseen class starts at the slowest known rate: its first launch can only come out
+    // shorter than planned, never several times longer
+    double r = msps_default_;
+    for (const auto& kv : class_msps_) r = std::min(r, kv.second);
+    return r;
 }
 
 // Samples of each admitted job (in admission order) for the next launch; 0 leaves a job out. The
@@ -373,17 +378,17 @@ void Server::worker() {
         // small jobs is dominated by its ramp-up and tail, and its low rate would shrink every
         // following slice (large jobs would then crawl through many short launches).
         // Refine the rates: each class in the launch moves by the ratio of predicted to measured
-        // time, weighted by its share of the prediction (a launch holding one class corrects it
-        // fully over a few launches; minor members barely move).
+        // time, to the power of its share of the prediction (a launch holding one class corrects it
+        // at once; minor members barely move).
         double pred = 0.0;
         for (double v : done.pred_ms) pred += v;
         if (done.err.empty() && ms > 0.f && pred >= 0.5 * cfg_.launch_target_ms) {
-            const double ratio = std::clamp(pred / (double)ms, 0.25, 4.0);
+            const double ratio = std::clamp(pred / (double)ms, 0.1, 10.0);
             std::map<uint64_t, double> share;
             for (size_t i = 0; i < done.jobs.size(); ++i) share[done.jobs[i]->rate_key] += done.pred_ms[i] / pred;
-            for (const auto& [key, w] : share) class_msps_[key] = class_rate(key) * std::pow(ratio, 0.5 * w);
-            const double rate = (double)done.samples / ((double)ms * 1e3);  // Msamples/s over every class
-            msps_default_ = 0.7 * msps_default_ + 0.3 * rate;
+            std::map<uint64_t, double> next;
+            for (const auto& [key, w] : share) next[key] = class_rate(key) * std::pow(ratio, w);
+            for (const auto& [key, r] : next) class_msps_[key] = r;
         }
         // Jobs this launch finished go to the download thread: no later launch touches their films,
         // so the copies overlap the launch in flight and the worker goes on enqueueing.

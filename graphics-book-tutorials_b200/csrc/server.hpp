@@ -88,8 +88,9 @@ private:
     uint64_t bytes_in_use_ = 0, peak_bytes_ = 0;
     // Rendering rate (Msamples/s) per job class -- scene content and depth limit: the mix's classes
     // differ several-fold (a 36-triangle box at depth 4 against 164k triangles at depth 8), so one
-    // rate for all would size launches for the last class that ran. Unseen classes start at
-    // msps_default_ (all launches' overall rate). Refined by launches that filled half their budget.
+    // rate for all would size launches for the last class that ran. Unseen classes start at the
+    // slowest known class rate (msps_default_ before any). Refined by launches that filled half their
+    // budget.
     std::map<uint64_t, double> class_msps_;
     double msps_default_ = 500.0;
     double class_rate(uint64_t key) const;
