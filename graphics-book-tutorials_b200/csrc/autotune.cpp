@@ -11,7 +11,7 @@
 //               x min_active in {8, 16, 24} at leaf_batch 8; stage 2, the stage-1 winner with
 //               leaf_batch in {4, 12, 16, 32}
 //   wavefront:  stage 1, paths in flight in {the largest pool that fits the persisting L2 set-aside
-//               (its launches carry a persisting access-policy window), 2M, 4M, 8M} (each capped at 64
+//               (its launches carry a persisting access-policy window), 2M, 4M, 8M, 16M} (each capped at 64
 //               per pixel, duplicates probed once) x register cap {10, 8} CTAs per SM; stage 2,
 //               min_active {16, 24}; probed with enough samples that the largest pool turns over about
 //               twice (8 to 64 per pixel). Queue capacity is
@@ -104,7 +104,7 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
         // effective pool sizes (the engine caps a pool at 64 slots per pixel), each probed once
         std::vector<int> pools;
         const int l2_pool = (int)wavefront_l2_resident_paths(dev);
-        for (long long want : {(long long)l2_pool, 1ll << 21, 1ll << 22, 1ll << 23}) {
+        for (long long want : {(long long)l2_pool, 1ll << 21, 1ll << 22, 1ll << 23, 1ll << 24}) {
             if (want < (1 << 16)) continue;
             const int eff = (int)std::max<long long>(32, std::min(want, 64 * pixels));
             if (std::find(pools.begin(), pools.end(), eff) == pools.end()) pools.push_back(eff);

@@ -23,7 +23,7 @@ def test_autotune_picks_valid_fastest_config(wfb, name, w, h):
     assert (t.block, t.occupancy) in {(128, 10), (128, 8), (128, 6), (128, 0), (64, 0), (256, 0)}
     assert t.min_active in (8, 16, 24) and t.leaf_batch in (4, 8, 12, 16, 32)
     facts = wfb.device_facts()
-    pools = {min(p, 64 * w * h) for p in (facts["wavefront_l2_resident_paths"], 1 << 21, 1 << 22, 1 << 23)}
+    pools = {min(p, 64 * w * h) for p in (facts["wavefront_l2_resident_paths"], 1 << 21, 1 << 22, 1 << 23, 1 << 24)}
     assert t.paths_in_flight in pools and t.wf_min_active in (16, 20, 24) and t.wf_occupancy in (8, 10)
     mk_only = wfb.autotune(scene, w, h, probe_spp=2, max_depth=8, try_wavefront=False)
     assert mk_only.mode == wfb.MEGAKERNEL and mk_only.paths_in_flight == 0 and mk_only.wavefront_msamples_s == 0
