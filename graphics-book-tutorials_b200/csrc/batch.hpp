@@ -38,6 +38,7 @@ public:
 
     int max_jobs() const { return max_jobs_; }
     const LaunchConfig& config() const { return cfg_; }
+    int resident_lanes() const { return resident_lanes_; }  // megakernel lanes or wavefront slots
     // Work units per pixel for a job of `pixels` pixels and `samples` samples.
     int chunks_for(int pixels, int samples) const;
     // Kernels launched by the last launch().

@@ -337,6 +337,13 @@ void Server::worker() {
                 f.pred_ms.push_back((double)sp.width * sp.height * sp.sample_count / (class_rate(j->rate_key) * 1e3));
                 JobBuffers b = j->buf;
                 b.chunks = std::min(b.chunks, sp.sample_count);
+                if (b.chunks > 1 && b.lbuf != nullptr) {
+                    // at least two work units per resident lane: a small image's slice is cut into
+                    // more, shorter units instead of a few long ones that leave the launch a tail
+                    const long long px = (long long)sp.width * sp.height;
+                    const long long want = (2ll * launchers_[0]->resident_lanes() + px - 1) / px;
+                    b.chunks = (int)std::min<long long>(sp.sample_count, std::max<long long>(b.chunks, want));
+                }
                 if (b.chunks > 1 && b.lbuf == nullptr) b.chunks = 1;
                 jobs.push_back(j);
                 tickets.push_back(f.tickets[i]);
@@ -377,17 +384,18 @@ void Server::worker() {
         // Only launches that filled most of their budget refine the rate: a launch carrying a few
         // small jobs is dominated by its ramp-up and tail, and its low rate would shrink every
         // following slice (large jobs would then crawl through many short launches).
-        // Refine the rates: each class in the launch moves by the ratio of predicted to measured
-        // time, to the power of its share of the prediction (a launch holding one class corrects it
-        // at once; minor members barely move).
+        // Refine the rates: each class in the launch moves toward the ratio of predicted to measured
+        // time, by half of it (at most 2x either way) to the power of its share of the prediction: a
+        // class converges over a few launches, and no single launch (a cold start, a tail) can move
+        // a rate far.
         double pred = 0.0;
         for (double v : done.pred_ms) pred += v;
         if (done.err.empty() && ms > 0.f && pred >= 0.5 * cfg_.launch_target_ms) {
-            const double ratio = std::clamp(pred / (double)ms, 0.1, 10.0);
+            const double ratio = std::clamp(pred / (double)ms, 0.5, 2.0);
             std::map<uint64_t, double> share;
             for (size_t i = 0; i < done.jobs.size(); ++i) share[done.jobs[i]->rate_key] += done.pred_ms[i] / pred;
             std::map<uint64_t, double> next;
-            for (const auto& [key, w] : share) next[key] = class_rate(key) * std::pow(ratio, w);
+            for (const auto& [key, w] : share) next[key] = class_rate(key) * std::pow(ratio, 0.5 * w);
             for (const auto& [key, r] : next) class_msps_[key] = r;
         }
         // Jobs this launch finished go to the download thread: no later launch touches their films,
