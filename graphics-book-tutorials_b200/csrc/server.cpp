@@ -63,6 +63,14 @@ Server::Server(const ServerConfig& cfg) : cfg_(cfg) {
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
         uint64_t keep = cfg_.budget_bytes;  // retain freed blocks in the pool between jobs
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        // Grow the pool once, up front: admission allocates each job's films while holding the
+        // server lock, and a pool that had to grow then (mapping new memory with persistent
+        // launches in flight) stalled the worker and every submit for 0.2-0.8 s on a B200.
+        const uint64_t warm = std::min<uint64_t>(cfg_.budget_bytes, kServerPrewarmBytes);
+        void* p = nullptr;
+        if (cudaMallocAsync(&p, warm, stream_) == cudaSuccess) cudaFreeAsync(p, stream_);
+        cudaGetLastError();  // a pool that cannot grow that far is not an error here
+        cudaStreamSynchronize(stream_);
     }
     thread_ = std::thread([this] { worker(); });
     dl_thread_ = std::thread([this] { downloader(); });

@@ -28,6 +28,10 @@ struct ServerConfig {
 // samples per launch, and at lambda = 10 jobs/s on the 64-job mix 4 units per pixel gave the lowest
 // p50/p95/p99 on a B200 (one-sample units: p95 3.5x higher; whole-pixel units: p95 1.4x higher).
 constexpr int kServerSplitChunks = 4;
+// Device memory the server reserves in the stream-ordered pool when it starts (within its budget):
+// room for the films and per-sample buffers of several large jobs at once (a 1920x1080, 64-spp job
+// holds about 1.6 GB).
+constexpr uint64_t kServerPrewarmBytes = 8ull << 30;
 
 enum JobState : int { kQueued = 0, kActive = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
 
