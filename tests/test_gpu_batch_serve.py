@@ -119,7 +119,8 @@ def test_batch_rejects_overfull_and_bad_jobs(wfb, scenes):
 
 
 @pytest.mark.parametrize("kw", [dict(fixed_slice=2), dict(launch_target_ms=1.0), dict(one_job_per_launch=True),
-                                dict(use_graph=False, fixed_slice=3)])
+                                dict(use_graph=False, fixed_slice=3), dict(launch_target_ms=1.0, schedule="shared"),
+                                dict(launch_target_ms=0.2, schedule="express")])
 def test_served_jobs_equal_solo_renders(wfb, scenes, kw):
     jobs = small_jobs(wfb, scenes, 10, seed=11)
     srv = wfb.Server(**kw)
