@@ -63,17 +63,10 @@ Server::Server(const ServerConfig& cfg) : cfg_(cfg) {
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
         uint64_t keep = cfg_.budget_bytes;  // retain freed blocks in the pool between jobs
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-        // Grow the pool once, up front: admission allocates each job's films while holding the
-        // server lock, and a pool that had to grow then (mapping new memory with persistent
-        // launches in flight) stalled the worker and every submit for 0.2-0.8 s on a B200.
-        const uint64_t warm = std::min<uint64_t>(cfg_.budget_bytes, kServerPrewarmBytes);
-        void* p = nullptr;
-        if (cudaMallocAsync(&p, warm, stream_) == cudaSuccess) cudaFreeAsync(p, stream_);
-        cudaGetLastError();  // a pool that cannot grow that far is not an error here
-        cudaStreamSynchronize(stream_);
     }
     thread_ = std::thread([this] { worker(); });
     dl_thread_ = std::thread([this] { downloader(); });
+    alloc_thread_ = std::thread([this] { allocator(); });
 }
 
 Server::~Server() { shutdown(); }
@@ -86,8 +79,10 @@ void Server::shutdown() {
     }
     cv_work_.notify_all();
     cv_dl_.notify_all();
+    cv_alloc_.notify_all();
     if (thread_.joinable()) thread_.join();
     if (dl_thread_.joinable()) dl_thread_.join();
+    if (alloc_thread_.joinable()) alloc_thread_.join();
     std::lock_guard<std::mutex> lock(mu_);
     for (auto& kv : jobs_)
         if (kv.second->mem) {
@@ -212,7 +207,7 @@ ServerStats Server::stats() {
     s.wall_s = t_first_ < 0 ? 0.0 : now_seconds() - t_first_;
     s.bytes_in_use = bytes_in_use_;
     s.peak_bytes = peak_bytes_;
-    s.queued = (int)queue_.size();
+    s.queued = (int)(queue_.size() + allocating_.size());
     s.active = (int)active_.size();
     return s;
 }
@@ -227,30 +222,93 @@ void Server::reset_stats() {
     peak_bytes_ = bytes_in_use_;
 }
 
-// Moves queued jobs to the active set while budget and launch capacity allow (FIFO, no overtaking).
+// Moves queued jobs to the allocator while the budget and the launch's capacity allow (FIFO, no
+// overtaking): their bytes are reserved here, the memory itself comes from allocator().
 bool Server::admit_locked() {
     bool any = false;
-    while (!queue_.empty() && (int)active_.size() < max_active_) {
+    while (!alloc_blocked_ && !queue_.empty() && (int)(active_.size() + allocating_.size()) < max_active_) {
         Job& j = *jobs_[queue_.front()];
         if (bytes_in_use_ + j.bytes > cfg_.budget_bytes) break;
-        const uint64_t p = (uint64_t)j.spec.width * j.spec.height;
-        j.buf.chunks = launchers_[0]->chunks_for((int)p, j.spec.sample_count);
-        if (cudaMallocAsync(&j.mem, j.bytes, stream_) != cudaSuccess) {
-            cudaGetLastError();
-            break;  // try again after a job retires
-        }
-        float* f = static_cast<float*>(j.mem);
-        j.buf.film = DevFilm{f, f + 3 * p, f + 4 * p, (int)p};
-        j.buf.lbuf = j.buf.chunks > 1 ? f + 5 * p : nullptr;
-        cudaMemsetAsync(f, 0, 5 * p * sizeof(float), stream_);
         bytes_in_use_ += j.bytes;
         peak_bytes_ = std::max(peak_bytes_, bytes_in_use_);
-        j.state = kActive;
-        active_.push_back(queue_.front());
+        allocating_.push_back(queue_.front());
         queue_.pop_front();
         any = true;
     }
+    if (any) cv_alloc_.notify_one();
     return any;
+}
+
+// Allocates and zeroes the films of admitted jobs, in admission order, on its own stream and
+// without the server lock: growing the stream-ordered pool while persistent launches run took up to
+// 0.8 s for 1.6 GB on a B200, and done under the lock (as admission once did) it stalled the worker
+// and every submit meanwhile. A job becomes active once its memory is ready. The thread first grows
+// the pool to the budget (at most 80% of the free memory), which it then keeps (release threshold).
+void Server::allocator() {
+    cudaSetDevice(device_);
+    cudaStream_t s = nullptr;
+    const cudaError_t se = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (se == cudaSuccess) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            const uint64_t warm = std::min<uint64_t>(cfg_.budget_bytes, (uint64_t)(0.8 * (double)free_b));
+            void* p = nullptr;
+            if (warm > 0 && cudaMallocAsync(&p, warm, s) == cudaSuccess) cudaFreeAsync(p, s);
+            cudaStreamSynchronize(s);
+        }
+        cudaGetLastError();  // a pool that cannot grow that far is not an error here
+    }
+    for (;;) {
+        uint64_t ticket;
+        Job* j;
+        {
+            std::unique_lock<std::mutex> lock(mu_);
+            cv_alloc_.wait(lock, [&] { return stop_ || !allocating_.empty(); });
+            if (stop_) break;
+            ticket = allocating_.front();
+            j = jobs_[ticket].get();
+        }
+        const uint64_t p = (uint64_t)j->spec.width * j->spec.height;
+        void* mem = nullptr;
+        cudaError_t e = se;
+        if (e == cudaSuccess) e = cudaMallocAsync(&mem, j->bytes, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(mem, 0, 5 * p * sizeof(float), s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) cudaGetLastError();
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            allocating_.pop_front();
+            if (e != cudaSuccess) {
+                // no room now (or a failed allocation): back to the head of the queue until a job
+                // releases memory
+                if (mem) to_free_.push_back(mem);
+                bytes_in_use_ -= j->bytes;
+                if (j->state == kCancelled) {
+                    jobs_.erase(ticket);
+                } else {
+                    queue_.push_front(ticket);
+                    alloc_blocked_ = true;
+                }
+            } else if (j->state == kCancelled) {
+                to_free_.push_back(mem);
+                bytes_in_use_ -= j->bytes;
+                jobs_.erase(ticket);
+            } else {
+                j->mem = mem;
+                j->buf.chunks = launchers_[0]->chunks_for((int)p, j->spec.sample_count);
+                float* f = static_cast<float*>(mem);
+                j->buf.film = DevFilm{f, f + 3 * p, f + 4 * p, (int)p};
+                j->buf.lbuf = j->buf.chunks > 1 ? f + 5 * p : nullptr;
+                j->state = kActive;
+                active_.push_back(ticket);
+            }
+        }
+        cv_work_.notify_one();
+    }
+    if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
 }
 
 double Server::class_rate(uint64_t key) const {
@@ -502,6 +560,7 @@ void Server::release_idle_locked(bool worker) {
         if (j.mem) to_free_.push_back(j.mem);
         j.mem = nullptr;
         bytes_in_use_ -= j.bytes;
+        alloc_blocked_ = false;  // memory came back: a job that found no room may try again
         if (j.state == kCancelled) jobs_.erase(*it);
         it = active_.erase(it);
     }

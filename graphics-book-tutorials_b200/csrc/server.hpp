@@ -28,10 +28,6 @@ struct ServerConfig {
 // samples per launch, and at lambda = 10 jobs/s on the 64-job mix 4 units per pixel gave the lowest
 // p50/p95/p99 on a B200 (one-sample units: p95 3.5x higher; whole-pixel units: p95 1.4x higher).
 constexpr int kServerSplitChunks = 4;
-// Device memory the server reserves in the stream-ordered pool when it starts (within its budget):
-// room for the films and per-sample buffers of several large jobs at once (a 1920x1080, 64-spp job
-// holds about 1.6 GB).
-constexpr uint64_t kServerPrewarmBytes = 8ull << 30;
 
 enum JobState : int { kQueued = 0, kActive = 1, kDone = 2, kCancelled = 3, kFailed = 4 };
 
@@ -70,6 +66,7 @@ private:
     bool admit_locked();
     void release_idle_locked(bool worker = true);
     void downloader();
+    void allocator();
     std::vector<int> plan_launch(const std::vector<Job*>& act);
 
     ServerConfig cfg_;
@@ -86,6 +83,10 @@ private:
     bool stop_ = false;
     std::thread thread_;
     std::thread dl_thread_;               // copies finished films to the host
+    std::thread alloc_thread_;            // allocates admitted jobs' films (allocator())
+    std::condition_variable cv_alloc_;
+    std::deque<uint64_t> allocating_;     // admitted jobs waiting for their memory, in order
+    bool alloc_blocked_ = false;          // an allocation failed: admit again once memory returns
     std::condition_variable cv_dl_;
     std::deque<uint64_t> dl_queue_;
     std::vector<void*> to_free_;          // device memory released off the worker, freed by it
