@@ -237,7 +237,7 @@ class _CDeviceFacts(ctypes.Structure):
                 ("total_memory_bytes", ctypes.c_uint64), ("free_memory_bytes", ctypes.c_uint64),
                 ("l2_bytes", ctypes.c_uint64), ("persisting_l2_max_bytes", ctypes.c_uint64),
                 ("access_window_max_bytes", ctypes.c_uint64), ("wavefront_l2_resident_paths", ctypes.c_int),
-                ("wavefront_slot_bytes", ctypes.c_int)]
+                ("wavefront_slot_bytes", ctypes.c_int), ("persisting_l2_set_aside_bytes", ctypes.c_uint64)]
 
 
 def device_facts() -> dict:

@@ -190,6 +190,9 @@ int wfb_device_facts_get(wfb_device_facts* out) {
         out->access_window_max_bytes = (uint64_t)prop.accessPolicyMaxWindowSize;
         out->wavefront_l2_resident_paths = (int)wfb::wavefront_l2_resident_paths(dev);
         out->wavefront_slot_bytes = (int)wfb::wavefront_slot_bytes();
+        size_t set_aside = 0;
+        wfb::cuda_check(cudaDeviceGetLimit(&set_aside, cudaLimitPersistingL2CacheSize), "persisting L2 set-aside");
+        out->persisting_l2_set_aside_bytes = set_aside;
     });
 }
 

@@ -62,6 +62,7 @@ typedef struct {
     uint64_t l2_bytes, persisting_l2_max_bytes, access_window_max_bytes;
     int wavefront_l2_resident_paths;
     int wavefront_slot_bytes;
+    uint64_t persisting_l2_set_aside_bytes; /* this process's current set-aside (0 when no pool holds a window) */
 } wfb_device_facts;
 int wfb_device_facts_get(wfb_device_facts* out);
 

@@ -184,3 +184,10 @@ def test_l2_resident_pool_renders_the_same_film(wfb):
     big.set_l2_residency(1)
     assert big.l2_window_bytes() > 0
     assert np.array_equal(bits(big.render(params).rgb), bits(mk.rgb))
+    assert wfb.device_facts()["persisting_l2_set_aside_bytes"] > 0
+    # the set-aside goes back once no pool holds a window: later kernels get the whole L2 again
+    big.close()
+    r.close()
+    import gc
+    gc.collect()  # renderers of earlier tests still waiting for collection may hold small windowed pools
+    assert wfb.device_facts()["persisting_l2_set_aside_bytes"] == 0
