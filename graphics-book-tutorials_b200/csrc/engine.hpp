@@ -57,7 +57,13 @@ uint64_t mix_key(uint64_t h, const void* data, size_t bytes);
 void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream);
 // The same result converted on the host: only copy engines work on the device, so it never waits
 // for SMs held by a persistent kernel of another stream (the server's download thread uses it).
-void film_download_host(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream);
+// Reusable pinned host memory for film_download_host (owned and freed by its caller).
+struct PinnedStaging {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+void film_download_host(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream,
+                        PinnedStaging* staging = nullptr);
 
 // Same scene view with another camera / resolution (batch jobs and orbit cameras).
 DevScene with_camera(const DevScene& s, const wf::Camera& cam, int width, int height);

@@ -223,27 +223,51 @@ void film_download(const DevFilm& film, int spp_done, float* rgb, float* lum_var
     cuda_check(es, "cudaStreamSynchronize");
 }
 
-void film_download_host(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream) {
+void film_download_host(const DevFilm& film, int spp_done, float* rgb, float* lum_var, cudaStream_t stream,
+                        PinnedStaging* staging) {
     if (spp_done <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "spp_done must be positive");
     const size_t p = (size_t)film.pixels;
+    const bool contiguous = film.lum == film.rgb + 3 * p && film.lum2 == film.rgb + 4 * p;
+    const float *h_rgb = nullptr, *h_lum = nullptr, *h_lum2 = nullptr;
     std::vector<float> lum, lum2;
-    if (rgb) cuda_check(cudaMemcpyAsync(rgb, film.rgb, 3 * p * sizeof(float), cudaMemcpyDeviceToHost, stream), "download rgb");
-    if (lum_var) {
-        lum.resize(p);
-        lum2.resize(p);
-        cuda_check(cudaMemcpyAsync(lum.data(), film.lum, p * sizeof(float), cudaMemcpyDeviceToHost, stream), "download lum");
-        cuda_check(cudaMemcpyAsync(lum2.data(), film.lum2, p * sizeof(float), cudaMemcpyDeviceToHost, stream),
-                   "download lum2");
+    if (staging && contiguous) {
+        // the whole film in one copy into reused pinned memory: full copy-engine bandwidth and no
+        // page faults, where pageable destinations are staged by the driver a piece at a time
+        const size_t bytes = 5 * p * sizeof(float);
+        if (staging->bytes < bytes) {
+            if (staging->ptr) cudaFreeHost(staging->ptr);
+            staging->ptr = nullptr;
+            staging->bytes = 0;
+            cuda_check(cudaHostAlloc(&staging->ptr, bytes, cudaHostAllocDefault), "cudaHostAlloc download staging");
+            staging->bytes = bytes;
+        }
+        cuda_check(cudaMemcpyAsync(staging->ptr, film.rgb, bytes, cudaMemcpyDeviceToHost, stream), "download film");
+        const float* f = static_cast<const float*>(staging->ptr);
+        h_rgb = f;
+        h_lum = f + 3 * p;
+        h_lum2 = f + 4 * p;
+    } else {
+        if (rgb) cuda_check(cudaMemcpyAsync(rgb, film.rgb, 3 * p * sizeof(float), cudaMemcpyDeviceToHost, stream), "download rgb");
+        if (lum_var) {
+            lum.resize(p);
+            lum2.resize(p);
+            cuda_check(cudaMemcpyAsync(lum.data(), film.lum, p * sizeof(float), cudaMemcpyDeviceToHost, stream), "download lum");
+            cuda_check(cudaMemcpyAsync(lum2.data(), film.lum2, p * sizeof(float), cudaMemcpyDeviceToHost, stream),
+                       "download lum2");
+        }
+        h_rgb = rgb;
+        h_lum = lum.data();
+        h_lum2 = lum2.data();
     }
     cuda_check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
     // The reference's host loops (WVM/src/gpu/gpu_renderer.cu:319-336), as film_resolve does them.
     const float inv = 1.0f / (float)spp_done;
     if (rgb)
-        for (size_t i = 0; i < 3 * p; ++i) rgb[i] *= inv;
+        for (size_t i = 0; i < 3 * p; ++i) rgb[i] = h_rgb[i] * inv;
     if (lum_var)
         for (size_t i = 0; i < p; ++i) {
-            const double m = (double)lum[i] / (double)spp_done;
-            const double m2 = (double)lum2[i] / (double)spp_done;
+            const double m = (double)h_lum[i] / (double)spp_done;
+            const double m2 = (double)h_lum2[i] / (double)spp_done;
             lum_var[i] = (float)std::max(0.0, m2 - m * m);
         }
 }

@@ -502,6 +502,13 @@ void Server::downloader() {
     cudaSetDevice(device_);
     cudaStream_t dl_stream = nullptr;  // this thread's copies: ordered after nothing but themselves
     const cudaError_t se = cudaStreamCreateWithFlags(&dl_stream, cudaStreamNonBlocking);
+    // Pinned staging for the films, sized up front for a 1920x1080 film (grown if a larger one comes):
+    // pinning host memory while launches run is one more driver call that can wait.
+    PinnedStaging staging;
+    if (cudaHostAlloc(&staging.ptr, 5ull * 1920 * 1080 * sizeof(float), cudaHostAllocDefault) == cudaSuccess)
+        staging.bytes = 5ull * 1920 * 1080 * sizeof(float);
+    else
+        staging.ptr = nullptr, cudaGetLastError();
     for (;;) {
         uint64_t ticket;
         Job* j;
@@ -519,7 +526,8 @@ void Server::downloader() {
             j->rgb.resize(3 * p);
             j->lum_var.resize(p);
             cuda_check(se, "cudaStreamCreate download");
-            film_download_host(j->buf.film, j->spec.sample_count, j->rgb.data(), j->lum_var.data(), dl_stream);
+            film_download_host(j->buf.film, j->spec.sample_count, j->rgb.data(), j->lum_var.data(), dl_stream,
+                               &staging);
         } catch (const std::exception& e) {
             err = e.what();
         }
@@ -544,6 +552,7 @@ void Server::downloader() {
         cv_work_.notify_one();  // memory came back: more jobs may be admitted
     }
     if (dl_stream) cudaStreamDestroy(dl_stream);
+    if (staging.ptr) cudaFreeHost(staging.ptr);
 }
 
 // Releases jobs that left the active set (done, failed or cancelled) once no launch in flight
