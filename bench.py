@@ -209,7 +209,7 @@ def bench_batch(wfb, scenes, n_jobs=64, repeats=2):
     batch_ms = min(b.run().render_ms for _ in range(repeats))
     b.close()
     # the same batch on the other arm: every job's paths in one persistent wavefront pool
-    bw = wfb.Batch(max_jobs=n_jobs, mode=wfb.WAVEFRONT, paths_in_flight=1 << 22)
+    bw = wfb.Batch(max_jobs=n_jobs, mode=wfb.WAVEFRONT)
     for s, j in jobs:
         bw.add(s, j)
     bw.run()

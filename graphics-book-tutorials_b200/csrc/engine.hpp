@@ -175,11 +175,11 @@ void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
 
 // ---- wavefront (wavefront.cu) ----
 struct WavefrontConfig {
-    int paths_in_flight = 0;  // path-pool slots; 0: 8M (capped at 64 x pixels)
+    int paths_in_flight = 0;  // path-pool slots; 0: 16M (capped at 64 x pixels)
     int l2_persist = -1;      // pool under a persisting L2 window: -1 when it fits the set-aside, 0 never, 1 always
     int occupancy = 10;       // register cap for 6, 8 or 10 CTAs of 128 threads per SM (0: none)
     bool suspend_stragglers = true;  // carry the last extension rays of a bounce over to the next
-    int min_active = 20;      // traverse on while at least this many lanes of a warp traverse
+    int min_active = 24;      // traverse on while at least this many lanes of a warp traverse
     int leaf_batch = 8;       // a warp tests primitives once this many lanes hold a pending leaf
 };
 

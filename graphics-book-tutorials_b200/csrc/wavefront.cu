@@ -6,7 +6,7 @@
 // in one arena. A pool that fits the device's persisting L2 set-aside (about 180 B per slot, so a
 // few hundred thousand paths on a B200; wavefront_l2_resident_paths) runs under a persisting
 // access-policy window on every launch, so its state stays in L2 across bounces; larger pools (up
-// to 8M paths) stream through HBM. A slot owns a work unit (a pixel and a run of its samples, as in
+// to 16M paths, the default) stream through HBM. A slot owns a work unit (a pixel and a run of its samples, as in
 // the megakernel) and, when its path ends, regenerates the next sample of the same pixel or takes a
 // new unit: paths in flight stay constant until the work runs out. Film sums are kept per slot in
 // sample order (direct mode) or per (pixel, sample) in a buffer committed in order afterwards
@@ -718,7 +718,7 @@ size_t wavefront_l2_resident_paths(int device) {
 
 WavefrontEngine::WavefrontEngine(int pixels, const WavefrontConfig& cfg) : pixels_(pixels), cfg_(cfg) {
     if (pixels <= 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "wavefront needs at least one pixel");
-    int cap = cfg.paths_in_flight > 0 ? cfg.paths_in_flight : (1 << 23);
+    int cap = cfg.paths_in_flight > 0 ? cfg.paths_in_flight : (1 << 24);
     if (cap > pixels * 64) cap = pixels * 64;  // never more slots than units can use
     if (cap < 32) cap = 32;
     capacity_ = cap;
@@ -866,7 +866,7 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
     a.pool = st.pool;
     a.capacity = capacity_;
     a.qcap = (p.queue_capacity > 0 && p.queue_capacity < capacity_) ? (uint32_t)p.queue_capacity : (uint32_t)capacity_;
-    a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
+    a.min_active = cfg_.min_active > 0 ? cfg_.min_active : WavefrontConfig{}.min_active;
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = p.stage_timing ? 1 : 0;
     a.suspend = cfg_.suspend_stragglers ? 1 : 0;
@@ -901,7 +901,7 @@ int WavefrontEngine::run_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, 
     a.pool = state_->pool;
     a.capacity = capacity_;
     a.qcap = (uint32_t)capacity_;
-    a.min_active = cfg_.min_active > 0 ? cfg_.min_active : 20;
+    a.min_active = cfg_.min_active > 0 ? cfg_.min_active : WavefrontConfig{}.min_active;
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = 0;
     a.suspend = cfg_.suspend_stragglers ? 1 : 0;

@@ -224,7 +224,7 @@ typedef struct {
                             and wavefront (128-thread blocks; < 0: 10) */
     int min_active;      /* 1..32; <= 0: default */
     int leaf_batch;      /* 1..32; <= 0: default (see wfb_renderer_configure) */
-    int paths_in_flight; /* wavefront pool slots; <= 0: 8M */
+    int paths_in_flight; /* wavefront pool slots; <= 0: 16M */
     int split_chunks;    /* megakernel: work units per pixel of each job; <= 0: automatic (one
                             sample per unit while the job's per-sample buffer fits) */
 } wfb_launch_config;
