@@ -203,6 +203,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_renderer_device_bytes": (u64, [vp]),
         "wfb_renderer_configure": (i32, [vp, i32, i32, i32, i32, i32, i32, i32]),
         "wfb_renderer_set_l2_residency": (i32, [vp, i32]),
+        "wfb_renderer_set_speculation": (i32, [vp, i32]),
+        "wfb_scene_boxes_nested": (i32, [vp, ctypes.POINTER(ctypes.c_int)]),
         "wfb_device_facts_get": (i32, [vp]),
         "wfb_renderer_l2_window_bytes": (u64, [vp]),
         "wfb_renderer_width": (i32, [vp]),
@@ -292,6 +294,12 @@ class Scene:
         h = ctypes.c_void_p()
         _check(lib.wfb_scene_create(ctypes.byref(d), finalize_bins, ctypes.byref(h)))
         return cls(h.value)
+
+    def boxes_nested(self) -> bool:
+        """True when the BVH's boxes nest, so closest-hit rays may traverse speculatively."""
+        v = ctypes.c_int(0)
+        _check(load_library().wfb_scene_boxes_nested(self._h, ctypes.byref(v)))
+        return bool(v.value)
 
     def info(self) -> SceneInfo:
         inf = SceneInfo()
@@ -429,6 +437,10 @@ class GpuRenderer:
 
     def l2_window_bytes(self) -> int:
         return int(load_library().wfb_renderer_l2_window_bytes(self._h))
+
+    def set_speculation(self, on: bool) -> None:
+        """Speculative traversal in both arms (on by default); films are the same bits either way."""
+        _check(load_library().wfb_renderer_set_speculation(self._h, int(bool(on))))
 
     def apply_tuning(self, tuning: "TuneResult") -> None:
         """Applies the knobs of an autotune result that belong to this renderer's arm."""

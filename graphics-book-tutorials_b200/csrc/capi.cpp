@@ -270,6 +270,13 @@ int wfb_scene_info_get(wfb_scene_t s, wfb_scene_info* info) {
     });
 }
 
+int wfb_scene_boxes_nested(wfb_scene_t s, int* nested) {
+    return guarded([&] {
+        need(s && nested, "null argument");
+        *nested = wfb::check_boxes_nested(s->host.nodes);
+    });
+}
+
 int wfb_scene_export(wfb_scene_t s, void* spheres, float* vertices, int* triangles, void* materials,
                      void* nodes, int* prim_order, void* lights) {
     return guarded([&] {
@@ -426,6 +433,13 @@ int wfb_renderer_set_l2_residency(wfb_renderer_t r, int mode) {
         need(r != nullptr, "null renderer");
         need(mode >= -1 && mode <= 1, "L2 residency mode must be -1, 0 or 1");
         r->r->set_l2_residency(mode);
+    });
+}
+
+int wfb_renderer_set_speculation(wfb_renderer_t r, int on) {
+    return guarded([&] {
+        need(r != nullptr, "null renderer");
+        r->r->set_speculation(on != 0);
     });
 }
 

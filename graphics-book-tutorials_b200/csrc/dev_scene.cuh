@@ -37,6 +37,9 @@ struct DevScene {
     wf::Vec3 env;
     wf::CameraRig camera;
     int width, height;
+    // 1 when every node's box lies inside the box of each node whose subtree holds it (checked at
+    // upload): the condition under which speculative closest-hit traversal is exact (box_step).
+    int boxes_nested;
 };
 
 constexpr int kLeafCountBits = 4;
@@ -150,6 +153,28 @@ struct TravRay {
 // query at the first hit. Splitting the steps lets a warp group them: rounds of box steps, and
 // rounds of primitive steps once enough lanes hold a pending leaf, instead of every box round
 // waiting while the one or two lanes that reached a leaf test its primitives one after another.
+//
+// Speculation (after Aila and Laine's speculative traversal, HPG 2009, made exact): a lane that
+// holds a pending leaf may go on taking box steps, against the current tmax, which does not yet
+// include that leaf's hits. The first leaf it reaches that way is not recorded: the step marks
+// `node` with kNodeHeld and the lane stops there; once the pending leaf is done, the mark is
+// cleared and the same node takes an ordinary box step, against the tmax preorder traversal has at
+// that point, which decides the leaf. So leaves are entered in preorder with preorder's tmax, one at
+// a time, and the hit is the same. What speculation adds is box steps on nodes that preorder
+// traversal would have culled with its smaller tmax; their leaves then fail that final step, for
+// the box test is monotone in tmax and in the box (a box inside another, tested with the same tmax,
+// passes only if the outer one does: per axis its slab distances lie inside the outer box's, IEEE
+// rounding being monotone) -- so a leaf that preorder traversal never reaches, because an
+// enclosing node failed, fails too. Two conditions make that hold: nested boxes (the scene's
+// `boxes_nested`), and finite 1/d (a zero direction component makes slab distances 0 * inf, whose
+// NaN mapping is not monotone in the box). Any-hit queries never lower tmax, so for them
+// speculation needs neither.
+constexpr int kNodeHeld = 1 << 30;
+
+__device__ __forceinline__ bool finite_inv(const TravRay& ray) {
+    return fmaxf(fmaxf(fabsf(ray.inv_d.x), fabsf(ray.inv_d.y)), fabsf(ray.inv_d.z)) < INFINITY;
+}
+
 __device__ __forceinline__ void box_step(const float4* __restrict__ nodes, int n_nodes, const wf::Vec3& o,
                                          const TravRay& ray, float tmax, int& node, int& pend) {
     // the whole 32-byte node in one 256-bit load (nodes are 32-byte aligned: a 256-byte aligned array
@@ -165,9 +190,12 @@ __device__ __forceinline__ void box_step(const float4* __restrict__ nodes, int n
         const int leaf = __float_as_int(nb.w);
         if (leaf < 0) {
             node = node + 1;
-        } else {
+        } else if (pend == 0) {
             node = skip;
             pend = leaf;
+        } else {
+            node |= kNodeHeld;  // speculative: decided again once the pending leaf is done
+            return;
         }
     }
     if (node >= n_nodes) node = -1;
@@ -194,7 +222,10 @@ __device__ __forceinline__ void prim_step(const float4* __restrict__ prims, int 
                                     wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
     }
     pend += (1 << kLeafCountBits) - 1;
-    if ((pend & kLeafCountMask) == 0) pend = 0;
+    if ((pend & kLeafCountMask) == 0) {
+        pend = 0;
+        if (node >= kNodeHeld) node -= kNodeHeld;  // a leaf held back by speculation takes its box step next
+    }
     if (hit) {
         h.t = t;
         h.prim = p;

@@ -126,6 +126,32 @@ void run_sections(std::initializer_list<std::function<void()>> sections, bool pa
 
 }  // namespace
 
+// 1 when the preorder skip-link tree is properly nested and every node's box lies inside the box
+// of each internal node whose subtree holds it -- the subtree of node i being the nodes after i and
+// before its skip link (the end of the array when the link is -1). A stack holds the enclosing
+// internal nodes; each node is checked against the innermost one: its box inside that node's box,
+// its own skip link not past that node's. Speculative traversal is exact under this condition
+// (dev_scene.cuh, box_step); a tree that fails it is traversed without speculation.
+int check_boxes_nested(const std::vector<wf::BvhNode>& nodes) {
+    const int nn = (int)nodes.size();
+    auto end_of = [&](int i) { return nodes[i].skip < 0 ? nn : nodes[i].skip; };
+    std::vector<int> stack;
+    for (int j = 0; j < nn; ++j) {
+        while (!stack.empty() && j >= end_of(stack.back())) stack.pop_back();
+        const wf::BvhNode& c = nodes[j];
+        if (!stack.empty()) {
+            const int p = stack.back();
+            const wf::BvhNode& q = nodes[p];
+            if (end_of(j) > end_of(p)) return 0;
+            if (!(c.lo.x >= q.lo.x && c.lo.y >= q.lo.y && c.lo.z >= q.lo.z && c.hi.x <= q.hi.x &&
+                  c.hi.y <= q.hi.y && c.hi.z <= q.hi.z))
+                return 0;
+        }
+        if (c.prim_count == 0) stack.push_back(j);
+    }
+    return 1;
+}
+
 uint64_t mix_key(uint64_t h, const void* data, size_t bytes) {
     const unsigned char* p = static_cast<const unsigned char*>(data);
     size_t i = 0;
@@ -150,6 +176,8 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
     const int np = (int)host.prim_order.size();
     const int nl = (int)host.lights.size();
     const long long n_prims = (long long)ns + nt;
+    // node indices stay below kNodeHeld, the traversal's speculation mark (dev_scene.cuh)
+    if (nn >= kNodeHeld) throw Error(WFB_ERR_UNSUPPORTED, "BVH has 2^30 nodes or more");
     for (const wf::Sphere& s : host.spheres)
         if (s.material < 0 || s.material >= nm) throw Error(WFB_ERR_INVALID_ARGUMENT, "sphere material index out of range");
     for (const wf::Triangle& t : host.triangles) {
@@ -198,6 +226,7 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
 
     // The four parts are packed on their own threads for large scenes; an error is reported from
     // the first part (in this order) that found one, as a serial pass would.
+    int nested = 0;
     auto pack_nodes = [&] {
         // Nodes: {lo, skip} {hi, leaf}.
         for (int i = 0; i < nn; ++i) {
@@ -217,6 +246,7 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
             nodes[2 * i] = f4(n.lo, i2f(n.skip));
             nodes[2 * i + 1] = f4(n.hi, i2f(leaf));
         }
+        nested = check_boxes_nested(host.nodes);
     };
     auto pack_prims = [&] {
         // Leaf primitive records in prim_order order.
@@ -315,6 +345,7 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
     d.camera = wf::make_camera_rig(host.camera, host.width, host.height);
     d.width = host.width;
     d.height = host.height;
+    d.boxes_nested = nested;
     return rs;
 }
 

@@ -50,6 +50,9 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host);
 // Folds `bytes` of `data` into the key `h` (multiply-xorshift over 8-byte words).
 uint64_t mix_key(uint64_t h, const void* data, size_t bytes);
 
+// 1 when speculative closest-hit traversal is exact on this BVH (nested boxes; device_scene.cu).
+int check_boxes_nested(const std::vector<wf::BvhNode>& nodes);
+
 // Film download in the GPU-arm convention (mean rgb, luminance variance), resolved on the device;
 // shared by renderers, batches and the server. Ordered after the work already queued on `stream`
 // (null: the calling thread's own stream, for a film whose writers have finished); returns once
@@ -86,7 +89,8 @@ struct MegakernelConfig {
     int min_active = 16;    // traverse on while at least this many lanes of a warp traverse
     int split_chunks = 0;   // work units per pixel; 0: one sample per unit while its buffer fits
     int occupancy = 10;     // block 128 only: 6, 8 or 10 caps registers for that many CTAs per SM (0: none)
-    int leaf_batch = 8;     // a warp tests primitives once this many lanes hold a pending leaf
+    int leaf_batch = 12;    // a warp tests primitives once this many lanes hold a pending leaf
+    bool speculate = true;  // lanes holding a pending leaf go on with box steps (box_step)
 };
 // Split mode keeps each path's radiance (3 floats) per (pixel, sample) until the ordered commit;
 // automatic splitting keeps that buffer under kSplitBufferBytes (renders above it run in sub-passes).
@@ -181,6 +185,7 @@ struct WavefrontConfig {
     bool suspend_stragglers = true;  // carry the last extension rays of a bounce over to the next
     int min_active = 24;      // traverse on while at least this many lanes of a warp traverse
     int leaf_batch = 8;       // a warp tests primitives once this many lanes hold a pending leaf
+    bool speculate = true;    // lanes holding a pending leaf go on with box steps (box_step)
 };
 
 // Launch configuration of a batch or a server: the arm and its knobs.
@@ -232,6 +237,8 @@ public:
     void set_l2_residency(int mode);
     // Bytes of the wavefront pool under the window (0: none, or a megakernel renderer).
     uint64_t l2_window_bytes() const;
+    // Speculative traversal in both arms (box_step): films are the same bits either way.
+    void set_speculation(bool on);
 
 private:
     void alloc_film();

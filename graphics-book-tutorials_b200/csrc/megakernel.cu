@@ -22,7 +22,9 @@
 //    `min_active` lanes traverse; only then does it shade the lanes whose ray finished and give
 //    them their next ray (extension, the pending shadow ray of a Lambertian bounce, or the camera
 //    ray of the next sample) -- the "dynamic ray fetch" of Aila and Laine (HPG 2009) with
-//    one-lane-per-path shading.
+//    one-lane-per-path shading. A lane holding a pending leaf also takes part in box rounds until
+//    it reaches its next leaf (speculation, made exact in box_step), so box rounds stay full while
+//    leaves gather for a primitive round.
 //  * Film order: a unit is one pixel and a run of its samples in ascending order. Direct mode: a
 //    unit covers all samples of the pixel; the lane adds every finished path to register copies of
 //    the film sums (film_add order, WVM/src/gpu/engine.cuh:25-32). Split mode (a job with fewer
@@ -52,6 +54,7 @@ struct MkArgs {
     int count_rays;
     int min_active;
     int leaf_batch;
+    int speculate;  // speculative traversal (box_step): 1 on, 0 off
 };
 
 template <bool MULTI>
@@ -115,6 +118,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
     // or p + n * eps for both the next extension ray and the shadow ray) with tmin = kRayEps. ----
     int node = -1;
     int pend = 0;  // pending leaf (box_step / prim_step)
+    bool spec = false;  // this ray may take box steps while it holds a pending leaf (box_step)
     TravRay ray;
     wf::HitRecord h;
     h.t = 0.f;
@@ -126,11 +130,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
     int jn_nodes = 0, jn_spheres = 0;
     unsigned n_ext = 0, n_shadow = 0, n_invalid = 0, n_steps = 0, n_prims = 0;
 
-    auto start_ray = [&]() {
+    auto start_ray = [&](int boxes_nested) {
         const int nn = MULTI ? jn_nodes : a.job0.s.n_nodes;
         if (shadow_ray) traversal_begin(nn, sh_dir, sh_tmax, &ray, &node, &h);
         else traversal_begin(nn, ps.ray.d, ps.ray.tmax, &ray, &node, &h);
         pend = 0;
+        spec = a.speculate && (shadow_ray || (boxes_nested && finite_inv(ray)));
     };
     auto new_path = [&](const DevScene& s, uint32_t seed) {
         ps = wf::init_path(s, pixel % s.width, pixel / s.width, (uint32_t)sample, seed);
@@ -140,7 +145,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
         // ================= traversal: rounds of box steps or of primitive steps =================
         for (;;) {
             const bool in_leaf = pend != 0;
-            const bool at_box = node >= 0 && !in_leaf;
+            const bool at_box = node >= 0 && (!in_leaf || (spec && node < kNodeHeld));
             const unsigned pmask = __ballot_sync(kFull, in_leaf);
             const unsigned bmask = __ballot_sync(kFull, at_box);
             const unsigned tmask = pmask | bmask;
@@ -237,7 +242,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
                 }
             }
             if (pixel >= 0) {
-                start_ray();
+                start_ray(s.boxes_nested);
                 park();
             }
         }
@@ -292,7 +297,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
                     }
                     new_path(s, J.seed);
                     shadow_ray = false;
-                    start_ray();
+                    start_ray(s.boxes_nested);
                     park();
                 } else {
                     out_of_work = true;
@@ -474,6 +479,7 @@ int launch_megakernel(const DevScene& s, const DevFilm& film, DevCounters* count
     args.count_rays = p.count_rays ? 1 : 0;
     args.min_active = cfg.min_active;
     args.leaf_batch = cfg.leaf_batch;
+    args.speculate = cfg.speculate ? 1 : 0;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
     if (timer) timer->begin(stream);
     launch_any<false>(args, args.job0.units, cfg, args.job0.chunks > 1, stream);
@@ -496,6 +502,7 @@ void launch_megakernel_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, in
     args.count_rays = count_rays ? 1 : 0;
     args.min_active = cfg.min_active;
     args.leaf_batch = cfg.leaf_batch;
+    args.speculate = cfg.speculate ? 1 : 0;
     cuda_check(cudaMemsetAsync(work_counter, 0, sizeof(unsigned int), stream), "memset work counter");
     launch_any<true>(args, 0, cfg, all_split, stream);  // full persistent grid: the unit count lives on the device
     launch_film_commit_jobs(d_jobs, d_hdr, max_jobs, stream);

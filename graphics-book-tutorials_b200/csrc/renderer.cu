@@ -303,6 +303,12 @@ void Renderer::set_l2_residency(int mode) {
     wf_ = std::make_unique<Wavefront>(pixels(), wf_cfg_);
 }
 
+void Renderer::set_speculation(bool on) {
+    mk_cfg_.speculate = on;
+    wf_cfg_.speculate = on;
+    if (wf_) wf_->engine.set_speculate(on);
+}
+
 uint64_t Renderer::l2_window_bytes() const { return wf_ ? wf_->engine.l2_window_bytes() : 0; }
 
 uint64_t Renderer::device_bytes() const {

@@ -91,6 +91,7 @@ struct WfArgs {
     int leaf_batch;
     int split_shading;  // stage timing: a barrier between material queues
     int suspend;        // extension stragglers may be suspended to the next iteration
+    int speculate;      // speculative traversal (box_step)
     unsigned long long wait_ns;  // limit of every bounded wait (grid barriers, look-backs)
     unsigned bar_extra;          // CTAs a barrier waits for beyond the launch's own (0; 1 only in the
                                  // wait-timeout test, where no barrier can complete)
@@ -195,6 +196,7 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
     uint32_t id = 0;  // slot (extend) or shadow record (shadow) of the current ray
     int node = -1;
     int pend = 0;  // pending leaf (box_step / prim_step)
+    bool spec = false;  // the ray may take box steps while it holds a pending leaf (box_step)
     wf::Vec3 o{0.f, 0.f, 0.f};
     TravRay ray;
     wf::HitRecord h;
@@ -218,18 +220,21 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
                     id = SHADOW ? i : items[i];  // shadow records are numbered by queue position
                     // every ray starts at its path's origin with tmin = kRayEps (see TravRay)
                     const int slot = SHADOW ? __float_as_int(P.sh_c[id].w) : (int)id;
+                    int nested = a.job0.s.boxes_nested;
                     if (MULTI) {
                         const DevScene& js = a.jobs[P.unit[slot].w].s;
                         nodes = js.nodes;
                         prims = js.prims;
                         n_nodes = js.n_nodes;
                         n_spheres = js.n_spheres;
+                        nested = js.boxes_nested;
                     }
                     const float4 oo = P.ray_o[slot];
                     const float4 d = SHADOW ? P.sh_dir[id] : P.ray_d[id];
                     o = wf::Vec3{oo.x, oo.y, oo.z};
                     traversal_begin(n_nodes, wf::Vec3{d.x, d.y, d.z}, d.w, &ray, &node, &h);
                     pend = 0;
+                    spec = a.speculate && (SHADOW || (nested && finite_inv(ray)));
                     if (!SHADOW && P.alive[slot] == 2u) {  // resume a suspended ray where it stopped
                         const int2 tv = P.trav[slot];
                         const float4 hv = P.hit[slot];
@@ -252,7 +257,7 @@ __device__ void traverse_phase(const WfArgs& a, const uint32_t* items, unsigned 
         unsigned round = 0;
         for (;;) {
             const bool in_leaf = pend != 0;
-            const bool at_box = node >= 0 && !in_leaf;
+            const bool at_box = node >= 0 && (!in_leaf || (spec && node < kNodeHeld));
             const unsigned pm = __ballot_sync(kFull, in_leaf);
             const unsigned bm = __ballot_sync(kFull, at_box);
             const unsigned tm = pm | bm;
@@ -870,6 +875,7 @@ int WavefrontEngine::run(const DevScene& s, const DevFilm& film, DevCounters* co
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = p.stage_timing ? 1 : 0;
     a.suspend = cfg_.suspend_stragglers ? 1 : 0;
+    a.speculate = cfg_.speculate ? 1 : 0;
     int launches = launch_pool(st.kernel, a, st.grid, capacity_, counters, p.count_rays, st.window_bytes, st.hit_ratio,
                                       stream, timer);
     if (a.job0.chunks > 1) {
@@ -905,6 +911,7 @@ int WavefrontEngine::run_batch(const JobDesc* d_jobs, const BatchHeader* d_hdr, 
     a.leaf_batch = cfg_.leaf_batch > 0 ? cfg_.leaf_batch : 8;
     a.split_shading = 0;
     a.suspend = cfg_.suspend_stragglers ? 1 : 0;
+    a.speculate = cfg_.speculate ? 1 : 0;
     return launch_pool(state_->kernel_multi, a, state_->grid_multi, capacity_, counters, count_rays, state_->window_bytes,
                              state_->hit_ratio, stream);
 }

@@ -30,6 +30,8 @@ public:
     int capacity() const { return capacity_; }
     // Bytes of the pool under a persisting L2 access-policy window on every launch (0: none).
     size_t l2_window_bytes() const;
+    // Speculative traversal on or off for the following launches (box_step; same films either way).
+    void set_speculate(bool on) { cfg_.speculate = on; }
 
 private:
     struct State;

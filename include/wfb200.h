@@ -102,6 +102,10 @@ int wfb_scene_create(const wfb_scene_desc* desc, int finalize_bins, wfb_scene_t*
 int wfb_scene_generate(const char* name, int width, int height, uint32_t seed, int sah_bins,
                        wfb_scene_t* out);
 int wfb_scene_info_get(wfb_scene_t scene, wfb_scene_info* info);
+/* *nested = 1 when the scene's BVH is a properly nested preorder tree (every node's box inside the
+ * box of each node whose subtree -- the nodes before its skip link -- holds it): the condition for
+ * exact speculative closest-hit traversal (wfb_renderer_set_speculation). Host only. */
+int wfb_scene_boxes_nested(wfb_scene_t scene, int* nested);
 /* Copies the finalized host arrays into caller buffers sized from wfb_scene_info (any pointer
  * may be NULL to skip that array). */
 int wfb_scene_export(wfb_scene_t scene, void* spheres, float* vertices, int* triangles,
@@ -188,6 +192,12 @@ int wfb_renderer_configure(wfb_renderer_t r, int block, int blocks_per_sm, int m
 int wfb_renderer_set_l2_residency(wfb_renderer_t r, int mode);
 /* Bytes of the wavefront pool under the persisting window (0: none). */
 uint64_t wfb_renderer_l2_window_bytes(wfb_renderer_t r);
+/* Speculative traversal in both arms (no reference counterpart; on by default): a lane whose ray
+ * holds a leaf still to test goes on with box tests, and the next leaf it reaches is tested again
+ * once the first is done, so leaves are still entered in the reference's order and films are the
+ * same bits either way (WVM/include/wf/bvh.hpp:91-116). Closest-hit rays speculate only on a BVH
+ * whose boxes nest (wfb_scene_boxes_nested) and whose direction has no zero component. */
+int wfb_renderer_set_speculation(wfb_renderer_t r, int on);
 int wfb_renderer_width(wfb_renderer_t r);
 int wfb_renderer_height(wfb_renderer_t r);
 /* ~GpuRenderer. */

@@ -104,3 +104,47 @@ def test_parallel_bvh_build_is_identical_to_single_threaded(wfb, name, bins):
         e = s.export()
         out[threads] = (e["nodes"].tobytes(), e["prim_order"].tobytes(), s.hash())
     assert out[1] == out[3] == out[8]
+
+
+@pytest.mark.parametrize("name,bins", [("cornell36", 16), ("icospheres", 16), ("icospheres", 8)])
+def test_bvh_boxes_nest(wfb, name, bins):
+    """Speculative closest-hit traversal is exact on a nested tree; the builder's trees are nested."""
+    assert wfb.Scene.generate(name, 16, 9, 1234, bins).boxes_nested()
+
+
+@pytest.mark.slow
+def test_heightfield_boxes_nest(wfb):
+    assert wfb.Scene.generate("heightfield", 16, 9, 1234, 16).boxes_nested()
+
+
+@pytest.mark.parametrize("name", ["cornell", "divergence", "trianglehv", "furnace"])
+def test_reference_trees_nest(ref, wfb, name):
+    assert wfb.Scene.from_arrays(ref.ref_make_scene(name, 32, 18)).boxes_nested()
+
+
+def _first_internal_child(nodes):
+    """(parent, child) with the child a node inside the parent's subtree."""
+    for i in range(len(nodes)):
+        if nodes[i]["prim_count"] == 0:
+            return i, i + 1
+    raise AssertionError("no internal node")
+
+
+def test_boxes_nested_check_rejects_bad_trees(wfb):
+    a = wfb.Scene.generate("icospheres", 16, 9, 1234, 16).export()
+    assert wfb.Scene.from_arrays(a).boxes_nested()
+    p, c = _first_internal_child(a["nodes"])
+    # a child box reaching out of its parent's box
+    bad = a["nodes"].copy()
+    bad[c]["hi"][0] = np.nextafter(bad[p]["hi"][0], np.float32(np.inf))
+    assert not wfb.Scene.from_arrays(dict(a, nodes=bad)).boxes_nested()
+    # a leaf box shrunk by the smallest step is still nested
+    ok = a["nodes"].copy()
+    leaf = int(np.flatnonzero(ok["prim_count"] > 0)[0])
+    ok[leaf]["hi"][0] = max(np.nextafter(ok[leaf]["hi"][0], np.float32(-np.inf)), ok[leaf]["lo"][0])
+    assert wfb.Scene.from_arrays(dict(a, nodes=ok)).boxes_nested()
+    # a skip link out of the parent's subtree (past the parent's own skip link)
+    bad = a["nodes"].copy()
+    q = next(i for i in range(len(bad)) if bad[i]["prim_count"] == 0 and 0 <= bad[i]["skip"] < len(bad) - 1)
+    bad[q + 1]["skip"] = bad[q]["skip"] + 1
+    assert not wfb.Scene.from_arrays(dict(a, nodes=bad)).boxes_nested()
