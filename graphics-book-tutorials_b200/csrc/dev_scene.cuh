@@ -175,6 +175,12 @@ __device__ __forceinline__ bool finite_inv(const TravRay& ray) {
     return fmaxf(fmaxf(fabsf(ray.inv_d.x), fabsf(ray.inv_d.y)), fabsf(ray.inv_d.z)) < INFINITY;
 }
 
+// A lane may take a box step: it has a node to test and no pending leaf, or it speculates and its
+// node is not a held leaf.
+__device__ __forceinline__ bool can_box_step(int node, int pend, bool spec) {
+    return node >= 0 && (pend == 0 || (spec && node < kNodeHeld));
+}
+
 __device__ __forceinline__ void box_step(const float4* __restrict__ nodes, int n_nodes, const wf::Vec3& o,
                                          const TravRay& ray, float tmax, int& node, int& pend) {
     // the whole 32-byte node in one 256-bit load (nodes are 32-byte aligned: a 256-byte aligned array

@@ -1,6 +1,8 @@
 // Scene upload: validation and repacking into the device layout described in dev_scene.cuh.
 // Host arithmetic in this file is compiled without contraction (-ffp-contract=off) so every
 // precomputed float equals the one the reference computes per ray.
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <exception>
 #include <functional>
@@ -96,32 +98,38 @@ uint64_t fold(uint64_t h, uint64_t w) {
     return h ^ (h >> 29);
 }
 
-// Runs the sections in order, or each on its own thread when `parallel`; rethrows the error of the
-// first section (in order) that failed.
-void run_sections(std::initializer_list<std::function<void()>> sections, bool parallel) {
-    if (!parallel) {
-        for (const auto& f : sections) f();
-        return;
-    }
-    const std::vector<std::function<void()>> fs(sections);
+// Runs the sections on up to `threads` threads (the caller's included), each thread taking the next
+// section in order; rethrows the error of the first section (in order) that failed, as a serial
+// pass would.
+void run_sections(const std::vector<std::function<void()>>& fs, int threads) {
     std::vector<std::exception_ptr> errs(fs.size());
-    std::vector<std::thread> threads;
-    for (size_t k = 1; k < fs.size(); ++k)
-        threads.emplace_back([&, k] {
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+        for (size_t k; (k = next.fetch_add(1)) < fs.size();) {
             try {
                 fs[k]();
             } catch (...) {
                 errs[k] = std::current_exception();
             }
-        });
-    try {
-        fs[0]();
-    } catch (...) {
-        errs[0] = std::current_exception();
-    }
-    for (auto& t : threads) t.join();
+        }
+    };
+    std::vector<std::thread> pool;
+    const int extra = std::min<int>(threads, (int)fs.size()) - 1;
+    for (int t = 0; t < extra; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
     for (const auto& e : errs)
         if (e) std::rethrow_exception(e);
+}
+
+// Splits [0, n) into ranges of at least `grain` items, at most `parts` of them, as sections.
+void add_ranges(std::vector<std::function<void()>>& fs, int n, int grain, int parts,
+                const std::function<void(int, int)>& body) {
+    const int k = std::max(1, std::min(parts, n / std::max(1, grain)));
+    for (int c = 0; c < k; ++c) {
+        const int lo = (int)((long long)n * c / k), hi = (int)((long long)n * (c + 1) / k);
+        fs.emplace_back([=, &body] { body(lo, hi); });
+    }
 }
 
 }  // namespace
@@ -224,12 +232,10 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
     float* tri_area = reinterpret_cast<float*>(stage + off[kTriArea]);
     float4* lights = reinterpret_cast<float4*>(stage + off[kLights]);
 
-    // The four parts are packed on their own threads for large scenes; an error is reported from
-    // the first part (in this order) that found one, as a serial pass would.
     int nested = 0;
-    auto pack_nodes = [&] {
+    const std::function<void(int, int)> pack_nodes = [&](int lo, int hi) {
         // Nodes: {lo, skip} {hi, leaf}.
-        for (int i = 0; i < nn; ++i) {
+        for (int i = lo; i < hi; ++i) {
             const wf::BvhNode& n = host.nodes[i];
             int leaf = -1;
             if (n.prim_count > 0) {
@@ -246,11 +252,10 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
             nodes[2 * i] = f4(n.lo, i2f(n.skip));
             nodes[2 * i + 1] = f4(n.hi, i2f(leaf));
         }
-        nested = check_boxes_nested(host.nodes);
     };
-    auto pack_prims = [&] {
+    const std::function<void(int, int)> pack_prims = [&](int lo, int hi) {
         // Leaf primitive records in prim_order order.
-        for (int j = 0; j < np; ++j) {
+        for (int j = lo; j < hi; ++j) {
             const int p = host.prim_order[j];
             if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "prim_order entry out of range");
             if (p < ns) {
@@ -267,9 +272,9 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
             }
         }
     };
-    auto pack_triangles = [&] {
+    const std::function<void(int, int)> pack_triangles = [&](int lo, int hi) {
         // Triangle shading records and areas.
-        for (int i = 0; i < nt; ++i) {
+        for (int i = lo; i < hi; ++i) {
             const wf::Triangle& t = host.triangles[i];
             const wf::Vec3 e1 = host.vertices[t.i1] - host.vertices[t.i0];
             const wf::Vec3 e2 = host.vertices[t.i2] - host.vertices[t.i0];
@@ -303,7 +308,16 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
             }
         }
     };
-    run_sections({pack_nodes, pack_prims, pack_triangles, pack_rest}, (size_t)nn + np + nt > (1u << 16));
+    // Sections in the order a serial pass would take: node ranges, the nesting check, primitive
+    // ranges, triangle ranges, the rest; large scenes spread them over up to 8 threads.
+    const int threads = (size_t)nn + np + nt > (1u << 16) ? (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    std::vector<std::function<void()>> sections;
+    add_ranges(sections, nn, 1 << 14, threads, pack_nodes);
+    sections.emplace_back([&] { nested = check_boxes_nested(host.nodes); });
+    add_ranges(sections, np, 1 << 14, threads, pack_prims);
+    add_ranges(sections, nt, 1 << 14, threads, pack_triangles);
+    sections.emplace_back(pack_rest);
+    run_sections(sections, threads);
 
     auto rs = std::make_shared<ResidentScene>();
     cuda_check(cudaGetDevice(&rs->device), "cudaGetDevice");

@@ -44,6 +44,12 @@ namespace wfb {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+// Box steps per box round: a lane that can still step after one takes up to this many in a row
+// before the warp votes again, so the round's ballots and choice are paid once per several steps
+// (B200, 1280x720x64, against one step per round: icospheres +12%, heightfield +14%; 6 and 8 were
+// slower than 4 on icospheres). Each lane's steps are the same ones, in the same order.
+constexpr int kBoxSteps = 4;
+constexpr int kBatchBoxSteps = 4;
 
 struct MkArgs {
     JobDesc job0;              // single-job launch
@@ -81,17 +87,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
     bool shadow_ray = false, alive_after_shadow = false;
     wf::Vec3 sh_dir{0.f, 0.f, 0.f}, sh_contrib{0.f, 0.f, 0.f};
     float sh_tmax = 0.f;
-    // Single-job launches park the state that only shading reads in shared memory while the lane's
-    // ray traverses (one word per field per lane, field-major so a warp's words are consecutive),
-    // so that the traversal loop keeps only the ray, its origin and the traversal state in
-    // registers: 1-3% on one scene. Batch launches keep it in registers: their several scenes' BVHs
-    // want the whole L1 (parking cost them up to 13% on a B200).
-    constexpr bool PARK = !MULTI;
-    constexpr int kParked = !PARK ? 1 : SPLIT ? 22 : 27;
+    // The state that only shading reads is parked in shared memory while the lane's ray traverses
+    // (one word per field per lane, field-major so a warp's words are consecutive), so that the
+    // traversal loop keeps only the ray, its origin and the traversal state in registers: 1-3% on
+    // one scene, about 1% on the 64-job batch (whose several BVHs share what is left of L1; with one
+    // box step per round parking cost batches up to 13%, with kBoxSteps it gains).
+    constexpr int kParked = SPLIT ? 22 : 27;
     __shared__ float parked[kParked * BLOCK];
     auto P = [&](int f) -> float& { return parked[f * BLOCK + threadIdx.x]; };
     auto park = [&]() {
-        if constexpr (!PARK) return;
         P(0) = ps.throughput.x; P(1) = ps.throughput.y; P(2) = ps.throughput.z;
         P(3) = ps.L.x; P(4) = ps.L.y; P(5) = ps.L.z;
         P(6) = __int_as_float(ps.depth); P(7) = __int_as_float(ps.specular); P(8) = ps.prev_pdf;
@@ -103,7 +107,6 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
         if (!SPLIT) { P(22) = acc_r; P(23) = acc_g; P(24) = acc_b; P(25) = acc_l; P(26) = acc_l2; }
     };
     auto unpark = [&]() {
-        if constexpr (!PARK) return;
         ps.throughput = wf::Vec3{P(0), P(1), P(2)};
         ps.L = wf::Vec3{P(3), P(4), P(5)};
         ps.depth = __float_as_int(P(6)); ps.specular = __float_as_int(P(7)); ps.prev_pdf = P(8);
@@ -145,7 +148,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
         // ================= traversal: rounds of box steps or of primitive steps =================
         for (;;) {
             const bool in_leaf = pend != 0;
-            const bool at_box = node >= 0 && (!in_leaf || (spec && node < kNodeHeld));
+            const bool at_box = can_box_step(node, pend, spec);
             const unsigned pmask = __ballot_sync(kFull, in_leaf);
             const unsigned bmask = __ballot_sync(kFull, at_box);
             const unsigned tmask = pmask | bmask;
@@ -164,9 +167,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) megakernel_persistent(const MkArg
                     else prim_step(a.job0.s.prims, a.job0.s.n_spheres, ps.ray.o, ray, shadow_ray, node, pend, h);
                 }
             } else if (at_box) {
-                if (COUNT) ++n_steps;
-                if (MULTI) box_step(jnodes, jn_nodes, ps.ray.o, ray, h.t, node, pend);
-                else box_step(a.job0.s.nodes, a.job0.s.n_nodes, ps.ray.o, ray, h.t, node, pend);
+#pragma unroll
+                for (int k = 0; k < (MULTI ? kBatchBoxSteps : kBoxSteps); ++k) {
+                    if (k == 0 || can_box_step(node, pend, spec)) {
+                        if (COUNT) ++n_steps;
+                        if (MULTI) box_step(jnodes, jn_nodes, ps.ray.o, ray, h.t, node, pend);
+                        else box_step(a.job0.s.nodes, a.job0.s.n_nodes, ps.ray.o, ray, h.t, node, pend);
+                    }
+                }
             }
         }
 

@@ -230,9 +230,9 @@ typedef struct {
     int mode;            /* WFB_MODE_MEGAKERNEL or WFB_MODE_WAVEFRONT */
     int use_graph;       /* megakernel: replay one captured CUDA graph per launch shape */
     int block;           /* megakernel: 64, 128 or 256 threads; <= 0: 128 */
-    int occupancy;       /* register cap for 0, 6, 8 or 10 CTAs per SM: megakernel (block 128; < 0: 8)
-                            and wavefront (128-thread blocks; < 0: 10) */
-    int min_active;      /* 1..32; <= 0: default */
+    int occupancy;       /* register cap for 0, 6, 8 or 10 CTAs per SM: megakernel (block 128) and
+                            wavefront (128-thread blocks); < 0: 10 */
+    int min_active;      /* 1..32; <= 0: default (megakernel batches and servers 12) */
     int leaf_batch;      /* 1..32; <= 0: default (see wfb_renderer_configure) */
     int paths_in_flight; /* wavefront pool slots; <= 0: 16M */
     int split_chunks;    /* megakernel: work units per pixel of each job; <= 0: automatic (one
