@@ -517,7 +517,8 @@ def main():
             "issue_lane_frac": (round(prof["issue_active_frac"] * prof["lanes_per_instr"] / 32.0, 4)
                                 if "issue_active_frac" in prof and "lanes_per_instr" in prof else None),
             "note": "traversal is issue-bound on an L2-resident BVH: issue_lane_frac = issue_active_frac x "
-                    "lanes_per_instr/32 is the fraction of the SMs' thread-instruction slots doing useful work",
+                    "lanes_per_instr/32 is the fraction of the SMs' thread-instruction slots filled (warp votes "
+                    "and round bookkeeping included, so fewer such instructions can lower it as the kernel speeds up)",
         },
         "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},

@@ -134,30 +134,41 @@ void add_ranges(std::vector<std::function<void()>>& fs, int n, int grain, int pa
 
 }  // namespace
 
-// 1 when the preorder skip-link tree is properly nested and every node's box lies inside the box
-// of each internal node whose subtree holds it -- the subtree of node i being the nodes after i and
-// before its skip link (the end of the array when the link is -1). A stack holds the enclosing
-// internal nodes; each node is checked against the innermost one: its box inside that node's box,
-// its own skip link not past that node's. Speculative traversal is exact under this condition
-// (dev_scene.cuh, box_step); a tree that fails it is traversed without speculation.
-int check_boxes_nested(const std::vector<wf::BvhNode>& nodes) {
-    const int nn = (int)nodes.size();
-    auto end_of = [&](int i) { return nodes[i].skip < 0 ? nn : nodes[i].skip; };
-    std::vector<int> stack;
-    for (int j = 0; j < nn; ++j) {
-        while (!stack.empty() && j >= end_of(stack.back())) stack.pop_back();
-        const wf::BvhNode& c = nodes[j];
-        if (!stack.empty()) {
-            const int p = stack.back();
-            const wf::BvhNode& q = nodes[p];
-            if (end_of(j) > end_of(p)) return 0;
-            if (!(c.lo.x >= q.lo.x && c.lo.y >= q.lo.y && c.lo.z >= q.lo.z && c.hi.x <= q.hi.x &&
-                  c.hi.y <= q.hi.y && c.hi.z <= q.hi.z))
-                return 0;
+// Nesting check of the internal nodes in [lo, hi): each one's children -- i + 1, then the skip
+// link of each child in turn, up to the node's own skip link (the end of the array when the link is
+// -1) -- must lie inside its box, move forward, and end exactly at its skip link. By transitivity
+// every node that traversal can reach only through a passed internal node then lies inside that
+// node's box, and leaving a subtree lands on its skip link. In a well-formed tree each node is the
+// child of one node, so the walks take fewer steps than there are nodes; more steps mean a tree that
+// is not one, and fail.
+bool boxes_nested_range(const wf::BvhNode* n, int nn, int lo, int hi) {
+    long long budget = nn;
+    for (int i = lo; i < hi; ++i) {
+        const wf::BvhNode& q = n[i];
+        if (q.prim_count != 0) continue;
+        const int end_i = q.skip < 0 ? nn : q.skip;
+        if (end_i <= i) return false;
+        int c = i + 1;
+        while (c < end_i) {
+            if (--budget < 0) return false;
+            const wf::BvhNode& k = n[c];
+            const int end_c = k.skip < 0 ? nn : k.skip;
+            if (end_c <= c || end_c > end_i) return false;
+            if (!(k.lo.x >= q.lo.x && k.lo.y >= q.lo.y && k.lo.z >= q.lo.z && k.hi.x <= q.hi.x &&
+                  k.hi.y <= q.hi.y && k.hi.z <= q.hi.z))
+                return false;
+            c = end_c;
         }
-        if (c.prim_count == 0) stack.push_back(j);
     }
-    return 1;
+    return true;
+}
+
+// 1 when the preorder skip-link tree is properly nested and every node's box lies inside the box
+// of each internal node whose subtree holds it (the subtree of node i: the nodes after i and before
+// its skip link). Speculative traversal is exact under this condition (dev_scene.cuh, box_step); a
+// tree that fails it is traversed without speculation.
+int check_boxes_nested(const std::vector<wf::BvhNode>& nodes) {
+    return boxes_nested_range(nodes.data(), (int)nodes.size(), 0, (int)nodes.size()) ? 1 : 0;
 }
 
 uint64_t mix_key(uint64_t h, const void* data, size_t bytes) {
@@ -313,11 +324,16 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
     const int threads = (size_t)nn + np + nt > (1u << 16) ? (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency())) : 1;
     std::vector<std::function<void()>> sections;
     add_ranges(sections, nn, 1 << 14, threads, pack_nodes);
-    sections.emplace_back([&] { nested = check_boxes_nested(host.nodes); });
+    std::atomic<int> nested_ok{1};
+    const std::function<void(int, int)> check_nested = [&](int lo, int hi) {
+        if (!boxes_nested_range(host.nodes.data(), nn, lo, hi)) nested_ok = 0;
+    };
+    add_ranges(sections, nn, 1 << 14, threads, check_nested);
     add_ranges(sections, np, 1 << 14, threads, pack_prims);
     add_ranges(sections, nt, 1 << 14, threads, pack_triangles);
     sections.emplace_back(pack_rest);
     run_sections(sections, threads);
+    nested = nested_ok.load();
 
     auto rs = std::make_shared<ResidentScene>();
     cuda_check(cudaGetDevice(&rs->device), "cudaGetDevice");
