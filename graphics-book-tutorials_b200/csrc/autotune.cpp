@@ -9,7 +9,7 @@
 // The result holds the best knobs of each arm, so a renderer of either arm can apply it.
 //   megakernel: stage 1, (block, occupancy target) in {(128,10), (128,8), (128,6), (128,0), (64,0), (256,0)}
 //               x min_active in {8, 16, 24} at leaf_batch 8; stage 2, the stage-1 winner with
-//               leaf_batch in {4, 12, 16, 32}
+//               leaf_batch in {4, 12, 16, 32}; stage 3, min_active 4 either side of the winner
 //   wavefront:  stage 1, paths in flight in {the largest pool that fits the persisting L2 set-aside
 //               (its launches carry a persisting access-policy window), 2M, 4M, 8M, 16M} (each capped at 64
 //               per pixel, duplicates probed once) x register cap {10, 8} CTAs per SM; stage 2,
@@ -94,6 +94,18 @@ TuneResult autotune(const std::shared_ptr<ResidentScene>& scene, const wf::Camer
             if (ms < mk_ms) {
                 mk_ms = ms;
                 best.leaf_batch = lb;
+            }
+        }
+        // stage 3: min_active 4 either side of the winner (the steps of stage 1 are 8 apart)
+        const int ma0 = best.min_active;
+        for (int ma : {ma0 - 4, ma0 + 4}) {
+            if (ma < 1 || ma > 32) continue;
+            r.configure(best.block, 0, ma, 0, -1, best.occupancy, best.leaf_batch);
+            const double ms = measure(r, p);
+            best.candidates++;
+            if (ms < mk_ms) {
+                mk_ms = ms;
+                best.min_active = ma;
             }
         }
     }

@@ -16,12 +16,12 @@ def test_autotune_picks_valid_fastest_config(wfb, name, w, h):
     scene = wfb.Scene.generate(name, w, h, 1234, 16)
     t = wfb.autotune(scene, w, h, probe_spp=2, max_depth=8, try_wavefront=True)
     assert t.mode in (wfb.MEGAKERNEL, wfb.WAVEFRONT)
-    assert t.candidates >= 18 + 4 + 2 + 2  # megakernel stages 1-2; wavefront pools x caps, min_active
+    assert t.candidates >= 18 + 4 + 1 + 2 + 2  # megakernel stages 1-3; wavefront pools x caps, min_active
     assert t.megakernel_msamples_s > 0 and t.wavefront_msamples_s > 0
     assert t.msamples_s == pytest.approx(max(t.megakernel_msamples_s, t.wavefront_msamples_s), rel=1e-9)
     assert (t.mode == wfb.WAVEFRONT) == (t.wavefront_msamples_s > t.megakernel_msamples_s)
     assert (t.block, t.occupancy) in {(128, 10), (128, 8), (128, 6), (128, 0), (64, 0), (256, 0)}
-    assert t.min_active in (8, 16, 24) and t.leaf_batch in (4, 8, 12, 16, 32)
+    assert t.min_active in (4, 8, 12, 16, 20, 24, 28) and t.leaf_batch in (4, 8, 12, 16, 32)
     facts = wfb.device_facts()
     pools = {min(p, 64 * w * h) for p in (facts["wavefront_l2_resident_paths"], 1 << 21, 1 << 22, 1 << 23, 1 << 24)}
     assert t.paths_in_flight in pools and t.wf_min_active in (16, 20, 24) and t.wf_occupancy in (8, 10)
