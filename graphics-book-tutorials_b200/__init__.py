@@ -205,6 +205,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_renderer_set_l2_residency": (i32, [vp, i32]),
         "wfb_renderer_set_speculation": (i32, [vp, i32]),
         "wfb_scene_boxes_nested": (i32, [vp, ctypes.POINTER(ctypes.c_int)]),
+        "wfb_test_traverse": (i32, [vp, vp, i32, i32, i32, i32, i32, vp]),
         "wfb_device_facts_get": (i32, [vp]),
         "wfb_renderer_l2_window_bytes": (u64, [vp]),
         "wfb_renderer_width": (i32, [vp]),
@@ -294,6 +295,17 @@ class Scene:
         h = ctypes.c_void_p()
         _check(lib.wfb_scene_create(ctypes.byref(d), finalize_bins, ctypes.byref(h)))
         return cls(h.value)
+
+    def test_traverse(self, rays: np.ndarray, anyhit: bool = False, speculate: bool = True, box_steps: int = 4,
+                      leaf_batch: int = 8) -> np.ndarray:
+        """Host run of the device traversal steps in simulated warps (wfb_test_traverse); rays of the
+        RAY dtype, hits of the HIT dtype."""
+        rays = np.ascontiguousarray(rays, RAY)
+        hits = np.zeros(rays.shape[0], HIT)
+        _check(load_library().wfb_test_traverse(self._h, rays.ctypes.data, int(rays.shape[0]), int(bool(anyhit)),
+                                                int(bool(speculate)), int(box_steps), int(leaf_batch),
+                                                hits.ctypes.data))
+        return hits
 
     def boxes_nested(self) -> bool:
         """True when the BVH's boxes nest, so closest-hit rays may traverse speculatively."""

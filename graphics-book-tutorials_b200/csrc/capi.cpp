@@ -270,6 +270,15 @@ int wfb_scene_info_get(wfb_scene_t s, wfb_scene_info* info) {
     });
 }
 
+int wfb_test_traverse(wfb_scene_t s, const void* rays, int n, int anyhit, int speculate, int box_steps,
+                      int leaf_batch, void* hits) {
+    return guarded([&] {
+        need(s && (n == 0 || (rays && hits)), "null argument");
+        wfb::traverse_check(s->host, static_cast<const float*>(rays), n, anyhit != 0, speculate != 0, box_steps,
+                            leaf_batch, static_cast<float*>(hits));
+    });
+}
+
 int wfb_scene_boxes_nested(wfb_scene_t s, int* nested) {
     return guarded([&] {
         need(s && nested, "null argument");

@@ -138,7 +138,8 @@ struct TravRay {
     wf::Vec3 d, inv_d;
 };
 
-// Resumable stackless skip-link traversal over the packed nodes, split into box steps and
+// Resumable stackless skip-link traversal over the packed nodes (the steps compile for the host
+// too: wfb_test_traverse runs them in simulated warps against the oracle), split into box steps and
 // primitive steps. A ray's whole traversal state is its next node (`node`, -1 when none is left),
 // its pending leaf (`pend`) and its best hit (`h`; h.t is the current tmax).
 //
@@ -171,29 +172,34 @@ struct TravRay {
 // speculation needs neither.
 constexpr int kNodeHeld = 1 << 30;
 
-__device__ __forceinline__ bool finite_inv(const TravRay& ray) {
+WF_HD bool finite_inv(const TravRay& ray) {
     return fmaxf(fmaxf(fabsf(ray.inv_d.x), fabsf(ray.inv_d.y)), fabsf(ray.inv_d.z)) < INFINITY;
 }
 
 // A lane may take a box step: it has a node to test and no pending leaf, or it speculates and its
 // node is not a held leaf.
-__device__ __forceinline__ bool can_box_step(int node, int pend, bool spec) {
+WF_HD bool can_box_step(int node, int pend, bool spec) {
     return node >= 0 && (pend == 0 || (spec && node < kNodeHeld));
 }
 
-__device__ __forceinline__ void box_step(const float4* __restrict__ nodes, int n_nodes, const wf::Vec3& o,
+WF_HD void box_step(const float4* __restrict__ nodes, int n_nodes, const wf::Vec3& o,
                                          const TravRay& ray, float tmax, int& node, int& pend) {
     // the whole 32-byte node in one 256-bit load (nodes are 32-byte aligned: a 256-byte aligned array
     // of 32-byte records); +0.9% on icospheres over two 128-bit loads, the same bits
     float4 na, nb;
+#if defined(__CUDA_ARCH__)
     asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
         : "=f"(na.x), "=f"(na.y), "=f"(na.z), "=f"(na.w), "=f"(nb.x), "=f"(nb.y), "=f"(nb.z), "=f"(nb.w)
         : "l"(nodes + 2 * node));
-    const int skip = __float_as_int(na.w);
+#else
+    na = nodes[2 * node];
+    nb = nodes[2 * node + 1];
+#endif
+    const int skip = f2i(na.w);
     if (!wf::hit_box_minmax(wf::Vec3{na.x, na.y, na.z}, wf::Vec3{nb.x, nb.y, nb.z}, o, ray.inv_d, wf::kRayEps, tmax)) {
         node = skip;
     } else {
-        const int leaf = __float_as_int(nb.w);
+        const int leaf = f2i(nb.w);
         if (leaf < 0) {
             node = node + 1;
         } else if (pend == 0) {
@@ -207,12 +213,12 @@ __device__ __forceinline__ void box_step(const float4* __restrict__ nodes, int n
     if (node >= n_nodes) node = -1;
 }
 
-__device__ __forceinline__ void prim_step(const float4* __restrict__ prims, int n_spheres, const wf::Vec3& o,
+WF_HD void prim_step(const float4* __restrict__ prims, int n_spheres, const wf::Vec3& o,
                                           const TravRay& ray, bool anyhit, int& node, int& pend, wf::HitRecord& h) {
     const float4* rec = prims + 3 * (pend >> kLeafCountBits);
-    const float4 q0 = __ldg(rec);
-    const float4 q1 = __ldg(rec + 1);
-    const int p = __float_as_int(q0.w);
+    const float4 q0 = ro_load(rec);
+    const float4 q1 = ro_load(rec + 1);
+    const int p = f2i(q0.w);
     wf::Ray r;
     r.o = o;
     r.d = ray.d;
@@ -223,7 +229,7 @@ __device__ __forceinline__ void prim_step(const float4* __restrict__ prims, int 
     if (p < n_spheres) {
         hit = wf::hit_sphere_core(wf::Vec3{q0.x, q0.y, q0.z}, q1.x, r, &t);
     } else {
-        const float4 q2 = __ldg(rec + 2);
+        const float4 q2 = ro_load(rec + 2);
         hit = wf::hit_triangle_core(wf::Vec3{q0.x, q0.y, q0.z}, wf::Vec3{q1.x, q1.y, q1.z},
                                     wf::Vec3{q2.x, q2.y, q2.z}, r, &t, &u, &v);
     }
@@ -245,7 +251,7 @@ __device__ __forceinline__ void prim_step(const float4* __restrict__ prims, int 
 }
 
 // intersect() prologue (WVM/include/wf/bvh.hpp:92-94): the ray's traversal state before step 0.
-__device__ __forceinline__ void traversal_begin(int n_nodes, wf::Vec3 d, float tmax, TravRay* ray, int* node,
+WF_HD void traversal_begin(int n_nodes, wf::Vec3 d, float tmax, TravRay* ray, int* node,
                                                 wf::HitRecord* h) {
     ray->d = d;
     ray->inv_d = wf::Vec3{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};

@@ -134,6 +134,44 @@ void add_ranges(std::vector<std::function<void()>>& fs, int n, int grain, int pa
 
 }  // namespace
 
+void pack_node(const wf::Scene& host, int i, float4* out) {
+    // {lo, skip} {hi, leaf}
+    const int nn = (int)host.nodes.size(), np = (int)host.prim_order.size();
+    const wf::BvhNode& n = host.nodes[i];
+    int leaf = -1;
+    if (n.prim_count > 0) {
+        if (n.prim_count > kMaxLeafPrims) throw Error(WFB_ERR_UNSUPPORTED, "BVH leaf holds more than 15 primitives");
+        if (n.prim_start < 0 || (long long)n.prim_start + n.prim_count > np || n.prim_start > kMaxLeafStart)
+            throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH leaf prim_start/count out of bounds");
+        leaf = (n.prim_start << kLeafCountBits) | n.prim_count;
+    }
+    if (n.skip < -1 || n.skip >= nn) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link out of bounds");
+    // Every traversal step moves forward (to N+1 or to a forward skip), so a traversal ends after at
+    // most n_nodes steps; a backward skip could loop forever and is rejected.
+    if (n.skip != -1 && n.skip <= i) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link does not point forward");
+    out[0] = f4(n.lo, i2f(n.skip));
+    out[1] = f4(n.hi, i2f(leaf));
+}
+
+void pack_prim(const wf::Scene& host, int j, float4* out) {
+    const int ns = (int)host.spheres.size();
+    const long long n_prims = (long long)ns + (long long)host.triangles.size();
+    const int p = host.prim_order[j];
+    if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "prim_order entry out of range");
+    if (p < ns) {
+        const wf::Sphere& s = host.spheres[p];
+        out[0] = f4(s.center, i2f(p));
+        out[1] = make_float4(s.radius, 0, 0, 0);
+        out[2] = make_float4(0, 0, 0, 0);
+    } else {
+        const wf::Triangle& t = host.triangles[p - ns];
+        const wf::Vec3 p0 = host.vertices[t.i0];
+        out[0] = f4(p0, i2f(p));
+        out[1] = f4(host.vertices[t.i1] - p0, 0.0f);
+        out[2] = f4(host.vertices[t.i2] - p0, 0.0f);
+    }
+}
+
 // Nesting check of the internal nodes in [lo, hi): each one's children -- i + 1, then the skip
 // link of each child in turn, up to the node's own skip link (the end of the array when the link is
 // -1) -- must lie inside its box, move forward, and end exactly at its skip link. By transitivity
@@ -245,43 +283,10 @@ std::shared_ptr<ResidentScene> upload_scene(const wf::Scene& host) {
 
     int nested = 0;
     const std::function<void(int, int)> pack_nodes = [&](int lo, int hi) {
-        // Nodes: {lo, skip} {hi, leaf}.
-        for (int i = lo; i < hi; ++i) {
-            const wf::BvhNode& n = host.nodes[i];
-            int leaf = -1;
-            if (n.prim_count > 0) {
-                if (n.prim_count > kMaxLeafPrims)
-                    throw Error(WFB_ERR_UNSUPPORTED, "BVH leaf holds more than 15 primitives");
-                if (n.prim_start < 0 || (long long)n.prim_start + n.prim_count > np || n.prim_start > kMaxLeafStart)
-                    throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH leaf prim_start/count out of bounds");
-                leaf = (n.prim_start << kLeafCountBits) | n.prim_count;
-            }
-            if (n.skip < -1 || n.skip >= nn) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link out of bounds");
-            // Every traversal step moves forward (to N+1 or to a forward skip), so a traversal ends
-            // after at most n_nodes steps; a backward skip could loop forever and is rejected.
-            if (n.skip != -1 && n.skip <= i) throw Error(WFB_ERR_INVALID_ARGUMENT, "BVH skip link does not point forward");
-            nodes[2 * i] = f4(n.lo, i2f(n.skip));
-            nodes[2 * i + 1] = f4(n.hi, i2f(leaf));
-        }
+        for (int i = lo; i < hi; ++i) pack_node(host, i, nodes + 2 * i);
     };
     const std::function<void(int, int)> pack_prims = [&](int lo, int hi) {
-        // Leaf primitive records in prim_order order.
-        for (int j = lo; j < hi; ++j) {
-            const int p = host.prim_order[j];
-            if (p < 0 || p >= n_prims) throw Error(WFB_ERR_INVALID_ARGUMENT, "prim_order entry out of range");
-            if (p < ns) {
-                const wf::Sphere& s = host.spheres[p];
-                prims[3 * j] = f4(s.center, i2f(p));
-                prims[3 * j + 1] = make_float4(s.radius, 0, 0, 0);
-                prims[3 * j + 2] = make_float4(0, 0, 0, 0);
-            } else {
-                const wf::Triangle& t = host.triangles[p - ns];
-                const wf::Vec3 p0 = host.vertices[t.i0];
-                prims[3 * j] = f4(p0, i2f(p));
-                prims[3 * j + 1] = f4(host.vertices[t.i1] - p0, 0.0f);
-                prims[3 * j + 2] = f4(host.vertices[t.i2] - p0, 0.0f);
-            }
-        }
+        for (int j = lo; j < hi; ++j) pack_prim(host, j, prims + 3 * j);
     };
     const std::function<void(int, int)> pack_triangles = [&](int lo, int hi) {
         // Triangle shading records and areas.

@@ -52,6 +52,14 @@ uint64_t mix_key(uint64_t h, const void* data, size_t bytes);
 
 // 1 when speculative closest-hit traversal is exact on this BVH (nested boxes; device_scene.cu).
 int check_boxes_nested(const std::vector<wf::BvhNode>& nodes);
+// Packed records (dev_scene.cuh layout) of node i (2 float4) and prim_order entry j (3 float4);
+// throw on what the traversal cannot use.
+void pack_node(const wf::Scene& host, int i, float4* out);
+void pack_prim(const wf::Scene& host, int j, float4* out);
+// Host run of the traversal steps in simulated 32-lane warps with the megakernel's round policy
+// (trav_check.cu): rays are {o, tmin, d, tmax} (tmin taken as kRayEps), hits {t, prim, u, v}.
+void traverse_check(const wf::Scene& host, const float* rays, int n, bool anyhit, bool speculate, int box_steps,
+                    int leaf_batch, float* hits);
 
 // Film download in the GPU-arm convention (mean rgb, luminance variance), resolved on the device;
 // shared by renderers, batches and the server. Ordered after the work already queued on `stream`

@@ -342,6 +342,14 @@ int wfb_scan_workspace_check(wfb_scan_workspace_t ws, void* stream);
  * claims the first scan tile): its waits run out after limit_ns, the kernel returns, and the call
  * reports WFB_ERR_DEVICE_WAIT (renders) or wfb_scan_workspace_check does. Process-wide. */
 int wfb_test_bounded_wait(uint64_t limit_ns, int unsatisfiable);
+/* Host-side check of the traversal steps (no reference counterpart; needs no GPU): the device's box
+ * and primitive steps, compiled for the host, run in simulated 32-lane warps with the megakernel's
+ * round choice -- a primitive round once leaf_batch lanes hold a pending leaf, else up to box_steps
+ * box steps per lane -- with speculation on or off. rays: n x {o[3], tmin, d[3], tmax} floats (tmin
+ * is taken as 1e-4, as every traced ray has it); hits: n x {t, prim (int bits), u, v}. The result
+ * equals preorder traversal (WVM/include/wf/bvh.hpp:91-116) whatever the knobs. */
+int wfb_test_traverse(wfb_scene_t scene, const void* rays, int n, int anyhit, int speculate, int box_steps,
+                      int leaf_batch, void* hits);
 
 /* ---- allocation-free rendering ---------------------------------------------------------------
  * No counterpart in the reference. For callers that must not allocate device memory on their
