@@ -236,12 +236,12 @@ def bench_batch(wfb, scenes, n_jobs=64, repeats=2):
 
 def sweep_batch(wfb, scenes, n_jobs=64):
     """Launch-shape sweep: the 64-job mix in one launch per configuration -- megakernel block
-    {64, 128, 256} and wavefront paths in flight {256K, 512K, 1M, 2M, 4M, 8M}. Yields one dict each."""
+    {64, 128, 256} and wavefront paths in flight {256K, 512K, 1M, 2M, 4M, 8M, 16M}. Yields one dict each."""
     mix = wfb.job_mix(n_jobs, SEED)
     jobs = [(scenes[m["scene"]], wfb.mix_job_desc(m, scenes[m["scene"]])) for m in mix]
     samples = sum(j.width * j.height * j.spp for _, j in jobs)
     configs = [dict(mode=wfb.MEGAKERNEL, block=b) for b in (64, 128, 256)] + \
-              [dict(mode=wfb.WAVEFRONT, paths_in_flight=1 << k) for k in range(18, 24)]
+              [dict(mode=wfb.WAVEFRONT, paths_in_flight=1 << k) for k in range(18, 25)]
     for cfg in configs:
         b = wfb.Batch(max_jobs=n_jobs, **cfg)
         for s, j in jobs:
