@@ -206,6 +206,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "wfb_renderer_set_speculation": (i32, [vp, i32]),
         "wfb_scene_boxes_nested": (i32, [vp, ctypes.POINTER(ctypes.c_int)]),
         "wfb_test_traverse": (i32, [vp, vp, i32, i32, i32, i32, i32, vp]),
+        "wfb_test_traverse_wide": (i32, [vp, vp, i32, i32, vp, vp]),
         "wfb_device_facts_get": (i32, [vp]),
         "wfb_renderer_l2_window_bytes": (u64, [vp]),
         "wfb_renderer_width": (i32, [vp]),
@@ -306,6 +307,16 @@ class Scene:
                                                 int(bool(speculate)), int(box_steps), int(leaf_batch),
                                                 hits.ctypes.data))
         return hits
+
+    def test_traverse_wide(self, rays: np.ndarray, anyhit: bool = False):
+        """Host model of a 4-wide traversal with re-tested speculation (wfb_test_traverse_wide): hits,
+        and counts {fetches, pops, retests, binary_steps}."""
+        rays = np.ascontiguousarray(rays, RAY)
+        hits = np.zeros(rays.shape[0], HIT)
+        counts = np.zeros(4, np.int64)
+        _check(load_library().wfb_test_traverse_wide(self._h, rays.ctypes.data, int(rays.shape[0]), int(bool(anyhit)),
+                                                     hits.ctypes.data, counts.ctypes.data))
+        return hits, dict(zip(("fetches", "pops", "retests", "binary_steps"), (int(c) for c in counts)))
 
     def boxes_nested(self) -> bool:
         """True when the BVH's boxes nest, so closest-hit rays may traverse speculatively."""

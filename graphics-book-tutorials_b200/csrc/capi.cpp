@@ -279,6 +279,15 @@ int wfb_test_traverse(wfb_scene_t s, const void* rays, int n, int anyhit, int sp
     });
 }
 
+int wfb_test_traverse_wide(wfb_scene_t s, const void* rays, int n, int anyhit, void* hits, int64_t* counts) {
+    return guarded([&] {
+        need(s && counts && (n == 0 || (rays && hits)), "null argument");
+        long long c[4] = {0, 0, 0, 0};
+        wfb::traverse_wide_check(s->host, static_cast<const float*>(rays), n, anyhit != 0, static_cast<float*>(hits), c);
+        for (int k = 0; k < 4; ++k) counts[k] = (int64_t)c[k];
+    });
+}
+
 int wfb_scene_boxes_nested(wfb_scene_t s, int* nested) {
     return guarded([&] {
         need(s && nested, "null argument");

@@ -60,6 +60,10 @@ void pack_prim(const wf::Scene& host, int j, float4* out);
 // (trav_check.cu): rays are {o, tmin, d, tmax} (tmin taken as kRayEps), hits {t, prim, u, v}.
 void traverse_check(const wf::Scene& host, const float* rays, int n, bool anyhit, bool speculate, int box_steps,
                     int leaf_batch, float* hits);
+// Host model of a 4-wide traversal with re-tested speculation over the same tree (trav_check.cu);
+// counts[4]: wide fetches, pops, re-tests after a tmax change, binary box steps of the same rays.
+void traverse_wide_check(const wf::Scene& host, const float* rays, int n, bool anyhit, float* hits,
+                         long long* counts);
 
 // Film download in the GPU-arm convention (mean rgb, luminance variance), resolved on the device;
 // shared by renderers, batches and the server. Ordered after the work already queued on `stream`

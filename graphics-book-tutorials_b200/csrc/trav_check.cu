@@ -89,4 +89,104 @@ void traverse_check(const wf::Scene& host, const float* rays, int n, bool anyhit
     }
 }
 
+
+// Host model of a 4-wide traversal over the same binary tree (a kernel to come): at an internal node
+// the boxes of its grandchildren (a leaf child stands for itself) are tested together against the
+// current tmax, and the passing ones go on a stack in reverse preorder with the tmax of that test;
+// a node taken off the stack is entered at once if tmax has not moved since (same tmax, same box
+// test), else tested again against the exact tmax. Middle nodes are never tested: a grandchild that
+// passes lies in its parent's box, which would have passed. On a nested tree with a finite 1/d
+// (the conditions of box_step's speculation) preorder traversal enters the same leaves in the same
+// order with the same tmax; other rays take the binary steps. counts: wide fetches (dependent loads
+// of a node's grandchild boxes), pops, re-tests after a tmax change, binary box steps of the same
+// rays (for comparison).
+void traverse_wide_check(const wf::Scene& host, const float* rays, int n, bool anyhit, float* hits,
+                         long long* counts) {
+    if (n < 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "bad traversal check arguments");
+    if (host.nodes.empty()) throw Error(WFB_ERR_NOT_FINALIZED, "Scene not finalized (no BVH nodes)");
+    const int nn = (int)host.nodes.size(), np = (int)host.prim_order.size();
+    if (nn >= kNodeHeld) throw Error(WFB_ERR_UNSUPPORTED, "BVH has 2^30 nodes or more");
+    std::vector<float4> nodes(2 * (size_t)nn), prims(3 * (size_t)(np > 0 ? np : 1));
+    for (int i = 0; i < nn; ++i) pack_node(host, i, &nodes[2 * (size_t)i]);
+    for (int j = 0; j < np; ++j) pack_prim(host, j, &prims[3 * (size_t)j]);
+    const bool nested = check_boxes_nested(host.nodes) != 0;
+    const int ns = (int)host.spheres.size();
+    auto end_of = [&](int i) {
+        const int skip = f2i(nodes[2 * (size_t)i].w);
+        return skip < 0 ? nn : skip;
+    };
+    auto leaf_of = [&](int i) { return f2i(nodes[2 * (size_t)i + 1].w); };
+    auto passes = [&](int i, const wf::Vec3& o, const TravRay& tr, float tmax) {
+        const float4 a = nodes[2 * (size_t)i], b = nodes[2 * (size_t)i + 1];
+        return wf::hit_box_minmax(wf::Vec3{a.x, a.y, a.z}, wf::Vec3{b.x, b.y, b.z}, o, tr.inv_d, wf::kRayEps, tmax);
+    };
+    long long fetches = 0, pops = 0, retests = 0, binary_steps = 0;
+    struct Entry {
+        int node;
+        float t;
+        bool tested;
+    };
+    std::vector<Entry> stack;
+    for (int k = 0; k < n; ++k) {
+        const float* r = rays + 8 * (size_t)k;
+        const wf::Vec3 o{r[0], r[1], r[2]};
+        TravRay tr;
+        wf::HitRecord h;
+        int node = 0, pend = 0;
+        // binary preorder steps: the fallback, and the comparison count
+        traversal_begin(nn, wf::Vec3{r[4], r[5], r[6]}, r[7], &tr, &node, &h);
+        const wf::HitRecord h0 = h;
+        while (node >= 0 || pend != 0) {
+            if (pend != 0) {
+                prim_step(prims.data(), ns, o, tr, anyhit, node, pend, h);
+            } else {
+                ++binary_steps;
+                box_step(nodes.data(), nn, o, tr, h.t, node, pend);
+            }
+        }
+        if (nested && finite_inv(tr)) {
+            h = h0;
+            stack.clear();
+            stack.push_back(Entry{0, 0.0f, false});
+            bool done = false;
+            while (!stack.empty() && !done) {
+                const Entry e = stack.back();
+                stack.pop_back();
+                ++pops;
+                if (!e.tested || e.t != h.t) {
+                    if (e.tested) ++retests;
+                    if (!passes(e.node, o, tr, h.t)) continue;
+                }
+                const int leaf = leaf_of(e.node);
+                if (leaf >= 0) {
+                    int p = leaf, dummy = 0;
+                    while (p != 0) prim_step(prims.data(), ns, o, tr, anyhit, dummy, p, h);
+                    done = anyhit && h.prim >= 0;
+                    continue;
+                }
+                ++fetches;
+                int cand[64], nc = 0;
+                for (int c = e.node + 1; c < end_of(e.node) && nc < 64; c = end_of(c)) {
+                    if (leaf_of(c) >= 0) {
+                        cand[nc++] = c;
+                        continue;
+                    }
+                    for (int g = c + 1; g < end_of(c) && nc < 64; g = end_of(g)) cand[nc++] = g;
+                }
+                for (int a = nc - 1; a >= 0; --a)
+                    if (passes(cand[a], o, tr, h.t)) stack.push_back(Entry{cand[a], h.t, true});
+            }
+        }
+        float* out = hits + 4 * (size_t)k;
+        out[0] = h.t;
+        std::memcpy(&out[1], &h.prim, 4);
+        out[2] = h.u;
+        out[3] = h.v;
+    }
+    counts[0] = fetches;
+    counts[1] = pops;
+    counts[2] = retests;
+    counts[3] = binary_steps;
+}
+
 }  // namespace wfb

@@ -350,6 +350,11 @@ int wfb_test_bounded_wait(uint64_t limit_ns, int unsatisfiable);
  * equals preorder traversal (WVM/include/wf/bvh.hpp:91-116) whatever the knobs. */
 int wfb_test_traverse(wfb_scene_t scene, const void* rays, int n, int anyhit, int speculate, int box_steps,
                       int leaf_batch, void* hits);
+/* Host model of a 4-wide traversal over the same tree (no reference counterpart; needs no GPU): the
+ * grandchildren of a node are box-tested together against the current tmax and stacked in preorder
+ * with that tmax; a node popped after tmax moved is tested again. Rays and hits as in
+ * wfb_test_traverse; counts[4]: wide fetches, pops, re-tests, binary box steps of the same rays. */
+int wfb_test_traverse_wide(wfb_scene_t scene, const void* rays, int n, int anyhit, void* hits, int64_t* counts);
 
 /* ---- allocation-free rendering ---------------------------------------------------------------
  * No counterpart in the reference. For callers that must not allocate device memory on their

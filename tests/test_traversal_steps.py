@@ -158,3 +158,34 @@ def test_traversal_steps_on_coplanar_quads(wfb, orc):
     for spec, steps, leaf_batch in [(True, 4, 12), (True, 1, 32), (True, 8, 32), (False, 4, 12)]:
         got = scene.test_traverse(rays, speculate=spec, box_steps=steps, leaf_batch=leaf_batch)
         assert _same(got, want), (spec, steps, leaf_batch)
+
+
+@pytest.mark.parametrize("name", ["icospheres", "cornell36", "trianglehv", "divergence"])
+@pytest.mark.parametrize("anyhit", [False, True])
+def test_wide_model_equals_preorder_traversal(wfb, orc, name, anyhit):
+    """The host model of a 4-wide traversal (grandchild boxes tested together, stacked with the tmax of
+    that test, re-tested when tmax has moved) enters the reference's leaves in the reference's order:
+    bit-equal hits on the adversarial rays, with far fewer dependent fetches than binary box steps."""
+    arrays = _scene(wfb, orc, name)
+    scene = wfb.Scene.from_arrays(arrays)
+    rays = _rays(wfb, arrays, 3000, seed=zlib.crc32(f"wide/{name}/{anyhit}".encode()))
+    want = orc.intersect(arrays, rays, anyhit=anyhit)
+    got, counts = scene.test_traverse_wide(rays, anyhit=anyhit)
+    assert _same(got, want)
+    if name == "icospheres" and not anyhit:
+        assert counts["fetches"] + counts["retests"] < 0.5 * counts["binary_steps"], counts
+
+
+def test_wide_model_on_coplanar_quads(wfb, orc):
+    scene, arrays = _coplanar_quads(wfb, seed=1)
+    rng = np.random.default_rng(2)
+    n = 100000
+    o = np.stack([rng.uniform(-3, 0.5, n), rng.uniform(-2, 2, n), rng.uniform(-2, 2, n)], 1)
+    tgt = np.stack([np.ones(n), rng.uniform(-1, 2, n), rng.uniform(-1, 2, n)], 1)
+    d = (tgt - o) / np.linalg.norm(tgt - o, axis=1, keepdims=True)
+    rays = np.zeros(n, wfb.RAY)
+    rays["o"], rays["d"] = o.astype(np.float32), d.astype(np.float32)
+    rays["tmin"], rays["tmax"] = np.float32(1e-4), np.float32(3.402823466e38)
+    got, counts = scene.test_traverse_wide(rays)
+    assert _same(got, orc.intersect(arrays, rays))
+    assert counts["retests"] > 0  # tmax moves between a stacked test and the pop on this scene
