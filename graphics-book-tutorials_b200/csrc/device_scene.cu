@@ -153,6 +153,49 @@ void pack_node(const wf::Scene& host, int i, float4* out) {
     out[1] = f4(n.hi, i2f(leaf));
 }
 
+bool pack_wide(const wf::Scene& host, std::vector<float4>* records, std::vector<int>* code_of) {
+    const int nn = (int)host.nodes.size();
+    auto end_of = [&](int i) { return host.nodes[i].skip < 0 ? nn : host.nodes[i].skip; };
+    auto is_leaf = [&](int i) { return host.nodes[i].prim_count > 0; };
+    std::vector<int> code(nn);
+    int n_wide = 0;
+    for (int i = 0; i < nn; ++i) {
+        const wf::BvhNode& n = host.nodes[i];
+        code[i] = is_leaf(i) ? ((n.prim_start << kLeafCountBits) | n.prim_count) : ~n_wide++;
+    }
+    std::vector<float4> rec(8 * (size_t)n_wide);
+    for (int i = 0; i < nn; ++i) {
+        if (is_leaf(i)) continue;
+        int cand[4], nc = 0;
+        for (int c = i + 1; c < end_of(i); c = end_of(c)) {
+            if (end_of(c) <= c) return false;
+            if (is_leaf(c)) {
+                if (nc == 4) return false;
+                cand[nc++] = c;
+                continue;
+            }
+            for (int g = c + 1; g < end_of(c); g = end_of(g)) {
+                if (end_of(g) <= g || nc == 4) return false;
+                cand[nc++] = g;
+            }
+        }
+        float4* r = &rec[8 * (size_t)~code[i]];
+        for (int k = 0; k < 4; ++k) {
+            if (k < nc) {
+                const wf::BvhNode& c = host.nodes[cand[k]];
+                r[2 * k] = f4(c.lo, i2f(cand[k]));
+                r[2 * k + 1] = f4(c.hi, i2f(code[cand[k]]));
+            } else {
+                r[2 * k] = make_float4(0, 0, 0, i2f(-1));
+                r[2 * k + 1] = make_float4(0, 0, 0, i2f(0));
+            }
+        }
+    }
+    records->swap(rec);
+    code_of->swap(code);
+    return true;
+}
+
 void pack_prim(const wf::Scene& host, int j, float4* out) {
     const int ns = (int)host.spheres.size();
     const long long n_prims = (long long)ns + (long long)host.triangles.size();

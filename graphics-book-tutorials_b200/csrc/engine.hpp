@@ -56,6 +56,12 @@ int check_boxes_nested(const std::vector<wf::BvhNode>& nodes);
 // throw on what the traversal cannot use.
 void pack_node(const wf::Scene& host, int i, float4* out);
 void pack_prim(const wf::Scene& host, int j, float4* out);
+// Wide records for a 4-wide traversal of the same tree: one per internal node, 8 float4 (128 B):
+// slot k = {lo, node id} {hi, code} for up to 4 candidates -- the node's grandchildren in preorder,
+// a leaf child standing for itself -- code = the candidate's leaf encoding (>= 0) or ~(its wide
+// record index) (< 0); an empty slot has node id -1. `code_of` gets each node's code. Returns false
+// (and leaves the outputs empty) when some internal node has more than 4 candidates.
+bool pack_wide(const wf::Scene& host, std::vector<float4>* records, std::vector<int>* code_of);
 // Host run of the traversal steps in simulated 32-lane warps with the megakernel's round policy
 // (trav_check.cu): rays are {o, tmin, d, tmax} (tmin taken as kRayEps), hits {t, prim, u, v}.
 void traverse_check(const wf::Scene& host, const float* rays, int n, bool anyhit, bool speculate, int box_steps,

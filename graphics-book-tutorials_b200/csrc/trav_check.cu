@@ -90,16 +90,16 @@ void traverse_check(const wf::Scene& host, const float* rays, int n, bool anyhit
 }
 
 
-// Host model of a 4-wide traversal over the same binary tree (a kernel to come): at an internal node
-// the boxes of its grandchildren (a leaf child stands for itself) are tested together against the
-// current tmax, and the passing ones go on a stack in reverse preorder with the tmax of that test;
-// a node taken off the stack is entered at once if tmax has not moved since (same tmax, same box
-// test), else tested again against the exact tmax. Middle nodes are never tested: a grandchild that
-// passes lies in its parent's box, which would have passed. On a nested tree with a finite 1/d
-// (the conditions of box_step's speculation) preorder traversal enters the same leaves in the same
-// order with the same tmax; other rays take the binary steps. counts: wide fetches (dependent loads
-// of a node's grandchild boxes), pops, re-tests after a tmax change, binary box steps of the same
-// rays (for comparison).
+// Host model of a 4-wide traversal over the same tree (a kernel to come), on the packed wide records
+// (pack_wide): at an internal node one 128-byte record holds the boxes of its grandchildren (a leaf
+// child stands for itself); they are tested together against the current tmax, and the passing ones
+// go on a stack in reverse preorder as (node id, code, tmax of that test). A node taken off the stack is
+// entered at once if tmax has not moved since (same tmax, same box test), else its own node record is
+// loaded and tested against the exact tmax. Middle nodes are never tested: a grandchild that passes
+// lies in its parent's box, which would have passed. On a nested tree with a finite 1/d (the
+// conditions of box_step's speculation) preorder traversal enters the same leaves in the same order
+// with the same tmax; other rays take the binary steps. counts: wide-record fetches, pops, re-tests
+// after a tmax change (node-record fetches), binary box steps of the same rays (for comparison).
 void traverse_wide_check(const wf::Scene& host, const float* rays, int n, bool anyhit, float* hits,
                          long long* counts) {
     if (n < 0) throw Error(WFB_ERR_INVALID_ARGUMENT, "bad traversal check arguments");
@@ -109,20 +109,14 @@ void traverse_wide_check(const wf::Scene& host, const float* rays, int n, bool a
     std::vector<float4> nodes(2 * (size_t)nn), prims(3 * (size_t)(np > 0 ? np : 1));
     for (int i = 0; i < nn; ++i) pack_node(host, i, &nodes[2 * (size_t)i]);
     for (int j = 0; j < np; ++j) pack_prim(host, j, &prims[3 * (size_t)j]);
+    std::vector<float4> wide;
+    std::vector<int> code_of;
+    const bool wide_ok = pack_wide(host, &wide, &code_of);
     const bool nested = check_boxes_nested(host.nodes) != 0;
     const int ns = (int)host.spheres.size();
-    auto end_of = [&](int i) {
-        const int skip = f2i(nodes[2 * (size_t)i].w);
-        return skip < 0 ? nn : skip;
-    };
-    auto leaf_of = [&](int i) { return f2i(nodes[2 * (size_t)i + 1].w); };
-    auto passes = [&](int i, const wf::Vec3& o, const TravRay& tr, float tmax) {
-        const float4 a = nodes[2 * (size_t)i], b = nodes[2 * (size_t)i + 1];
-        return wf::hit_box_minmax(wf::Vec3{a.x, a.y, a.z}, wf::Vec3{b.x, b.y, b.z}, o, tr.inv_d, wf::kRayEps, tmax);
-    };
     long long fetches = 0, pops = 0, retests = 0, binary_steps = 0;
     struct Entry {
-        int node;
+        int node, code;
         float t;
         bool tested;
     };
@@ -144,10 +138,10 @@ void traverse_wide_check(const wf::Scene& host, const float* rays, int n, bool a
                 box_step(nodes.data(), nn, o, tr, h.t, node, pend);
             }
         }
-        if (nested && finite_inv(tr)) {
+        if (wide_ok && nested && finite_inv(tr)) {
             h = h0;
             stack.clear();
-            stack.push_back(Entry{0, 0.0f, false});
+            stack.push_back(Entry{0, code_of[0], 0.0f, false});
             bool done = false;
             while (!stack.empty() && !done) {
                 const Entry e = stack.back();
@@ -155,26 +149,27 @@ void traverse_wide_check(const wf::Scene& host, const float* rays, int n, bool a
                 ++pops;
                 if (!e.tested || e.t != h.t) {
                     if (e.tested) ++retests;
-                    if (!passes(e.node, o, tr, h.t)) continue;
+                    const float4 a = nodes[2 * (size_t)e.node], b = nodes[2 * (size_t)e.node + 1];
+                    if (!wf::hit_box_minmax(wf::Vec3{a.x, a.y, a.z}, wf::Vec3{b.x, b.y, b.z}, o, tr.inv_d, wf::kRayEps,
+                                            h.t))
+                        continue;
                 }
-                const int leaf = leaf_of(e.node);
-                if (leaf >= 0) {
-                    int p = leaf, dummy = 0;
+                if (e.code >= 0) {  // a leaf: its primitives in leaf order
+                    int p = e.code, dummy = 0;
                     while (p != 0) prim_step(prims.data(), ns, o, tr, anyhit, dummy, p, h);
                     done = anyhit && h.prim >= 0;
                     continue;
                 }
                 ++fetches;
-                int cand[64], nc = 0;
-                for (int c = e.node + 1; c < end_of(e.node) && nc < 64; c = end_of(c)) {
-                    if (leaf_of(c) >= 0) {
-                        cand[nc++] = c;
-                        continue;
-                    }
-                    for (int g = c + 1; g < end_of(c) && nc < 64; g = end_of(g)) cand[nc++] = g;
+                const float4* w = &wide[8 * (size_t)~e.code];
+                for (int s = 3; s >= 0; --s) {
+                    const float4 lo = w[2 * s], hi = w[2 * s + 1];
+                    const int id = f2i(lo.w);
+                    if (id < 0) continue;
+                    if (wf::hit_box_minmax(wf::Vec3{lo.x, lo.y, lo.z}, wf::Vec3{hi.x, hi.y, hi.z}, o, tr.inv_d,
+                                           wf::kRayEps, h.t))
+                        stack.push_back(Entry{id, f2i(hi.w), h.t, true});
                 }
-                for (int a = nc - 1; a >= 0; --a)
-                    if (passes(cand[a], o, tr, h.t)) stack.push_back(Entry{cand[a], h.t, true});
             }
         }
         float* out = hits + 4 * (size_t)k;
